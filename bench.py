@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Benchmark: fitness evaluations per second (individual x atoms) of one GA generation.
+
+A step is one generation's fitness evaluation of the whole population over the
+whole training set (GPUGA's Fitness::compute, fitness.cu:316-333).  The default
+workload is the batched minimal-Tersoff Si set: 500 periodic diamond
+configurations of 8/64/216/512 atoms (~1e5 atoms), population 1000, seeded
+synthetic data (no public dataset exists for this path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours:       value = units / device time with populations resident in HBM
+            (gpuga_fitness_device); e2e = the same through gpuga_fitness with
+            host buffers (H2D population + D2H fitness inside the timed region).
+reference:  the reference's own implementation of this path, its CUDA build
+            (src/*.cu compiled unmodified into oracle/_ref/ref_probe), timing
+            Fitness::compute on the same workload and GPU.
+Multi-GPU (torchrun): every rank evaluates its own population of the same size
+(individuals are independent: weak scaling, no data-path collective); time is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fitness evals/s (indiv x atoms)"
+UNIT = "indiv*atoms/s"
+FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", type=int, default=2, choices=[1, 2, 3, 4])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-individuals", type=int, default=48)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- plumbing
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local_rank))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(prefix="gpuga_clocks_", suffix=".csv")
+        os.close(fd)
+        phys = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[self.device:self.device + 1]
+        idx = phys[0] if phys and phys[0] else str(self.device)
+        self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                      "-lms", "200", "-i", idx], stdout=open(self.path, "w"),
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+# ----------------------------------------------------------------------------- workload
+def oracle_evaluator():
+    from oracle import oracle
+
+    def evaluate(data, params):
+        d = tempfile.mkdtemp(prefix="gpuga_ref_t_")
+        from gpuga_b200 import synth
+        synth.write_dir(data, d)
+        s = oracle.OracleSet(d)
+        if int(data["potential_type"]) == 3:
+            s.set_nn2b(data.get("nn2b_r1", 7.0), data.get("nn2b_r2", 8.0), False)
+        out = s.find_force(params)
+        s.close()
+        shutil.rmtree(d, ignore_errors=True)
+        return out
+    return evaluate
+
+
+def engine_opts(data, device):
+    kw = dict(device=device)
+    if int(data["potential_type"]) == 3:
+        kw.update(nn2b_r1=float(data["nn2b_r1"]), nn2b_r2=float(data["nn2b_r2"]))
+    return kw
+
+
+def build_workload(workload: int, device: int):
+    """Synthetic set with teacher targets evaluated by the engine's own FP64 path."""
+    from gpuga_b200 import Fitness, synth
+    data = synth.make(workload)
+    with Fitness(arrays=data, **engine_opts(data, device)) as e0:
+        def evaluate(_data, params):
+            return e0.find_force64(params)
+        data = synth.fill_targets(data, evaluate)
+    return data, Fitness(arrays=data, **engine_opts(data, device))
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args, dist: Dist):
+    import torch
+
+    from gpuga_b200 import PATH_PLAIN64, _lib, synth
+    dev = dist.local_rank
+    torch.cuda.set_device(dev)
+    L = _lib.load()
+    data, e = build_workload(args.workload, dev)
+    P = int(data["ga"]["population_size"])
+    d = e.number_of_variables
+    Natoms = e.N
+    nsteps, nwarm = args.steps, max(args.warmup, 3)
+    pops_h = [synth.population(data, P, seed=1000 * dist.rank + k) for k in range(nsteps + nwarm)]
+    pops = torch.from_numpy(np.stack(pops_h)).to(f"cuda:{dev}")
+    fit = torch.empty(P, dtype=torch.float64, device=f"cuda:{dev}")
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dev}")
+    stream = torch.cuda.current_stream()
+    h = e.handle
+
+    def dev_step(k):
+        _lib.check(L.gpuga_fitness_device(h, P, C.c_void_p(pops[k].data_ptr()), C.c_void_p(fit.data_ptr()),
+                                          C.c_void_p(stream.cuda_stream)))
+
+    n_launch = C.c_int()
+    _lib.check(L.gpuga_plan_info(h, P, C.byref(n_launch), None, 0))
+    kernels_per_step = n_launch.value + 2  # + decode + fitness fold
+
+    # ---- value: device-resident inputs, device time per step, L2 flushed between steps
+    for k in range(nwarm):
+        dev_step(k)
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
+    for k in range(nsteps):
+        flush.zero_()
+        evs[k][0].record(stream)
+        dev_step(nwarm + k)
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = dist.max(sum(step_ms))
+    ms_per_step = total_ms / nsteps
+    value = dist.world * P * Natoms * nsteps / (total_ms / 1e3)
+    fit_dev = fit.cpu().numpy().copy()
+
+    # ---- per-launch device times (separate pass, launches bracketed by events on their own streams)
+    _lib.check(L.gpuga_kernel_timing(h, P, 1))
+    for k in range(nsteps):
+        flush.zero_()
+        dev_step(nwarm + k)
+    torch.cuda.synchronize()
+    rows = np.zeros((n_launch.value, 8))
+    _lib.check(L.gpuga_plan_info(h, P, None, C.c_void_p(rows.ctypes.data), n_launch.value))
+    _lib.check(L.gpuga_kernel_timing(h, P, 0))
+    peak_fp32 = C.c_double()
+    _lib.check(L.gpuga_calibrate_fp32(dev, C.byref(peak_fp32)))
+    kinds = {0: "tersoff_batched", 1: "pair_batched<RI>", 2: "pair_batched<NN2B>"}
+    launches = []
+    for r in rows:
+        launches.append({"kernel": f"{kinds[int(r[0])]}<{int(r[1])},{'force' if r[2] else 'energy_virial'}>",
+                         "ctas": int(r[3]), "units": r[4], "flops": r[5], "sfu_calls": r[6], "ms": r[7],
+                         "tflops": (r[5] / (r[7] * 1e-3) / 1e12) if r[7] > 0 else None})
+    dom = max(launches, key=lambda x: x["ms"])
+    roofline = {"bound": "fp32", "kernel": dom["kernel"], "achieved": dom["tflops"], "peak": peak_fp32.value,
+                "unit": "TFLOP/s", "frac": dom["tflops"] / peak_fp32.value if dom["tflops"] else None,
+                "traffic": None, "peak_source": "measured: FFMA-chain calibration kernel on this GPU",
+                "algorithmic": "FP32 flops of the batched formulation (FMA=2), transcendentals separate",
+                "ms_per_launch": dom["ms"], "launches": launches}
+
+    # ---- e2e through the public C ABI with host buffers
+    e2e_ms = []
+    out = np.zeros(P, np.float64)
+    for k in range(nwarm):
+        e.compute(P, pops_h[k], out)
+    dist.barrier()
+    for k in range(nsteps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _lib.check(L.gpuga_fitness(h, P, C.c_void_p(pops_h[nwarm + k].ctypes.data), C.c_void_p(out.ctypes.data)))
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_total = dist.max(sum(e2e_ms))
+    e2e_value = dist.world * P * Natoms * nsteps / (e2e_total / 1e3)
+    e2e_sorted = sorted(e2e_ms)
+    p50 = float(np.percentile(e2e_sorted, 50))
+    p99 = float(np.percentile(e2e_sorted, 99))
+
+    # ---- plain FP64 one-individual-per-launch path (denominator of the batched speed-up)
+    npl = min(args.plain_individuals, P)
+    plain_pop = pops_h[nwarm + nsteps - 1][:npl]
+    e.compute(1, plain_pop[:1], path=PATH_PLAIN64)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    fit64 = e.compute(npl, plain_pop, path=PATH_PLAIN64)
+    t_plain = time.perf_counter() - t0
+    plain_value = npl * Natoms / t_plain
+    batched = np.asarray(e.compute(P, pops_h[nwarm + nsteps - 1]))[:npl]
+    rel = np.abs(batched - fit64) / np.abs(fit64)
+    rank_same = bool(np.array_equal(np.argsort(batched, kind="stable"), np.argsort(fit64, kind="stable")))
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": nsteps, "warmup": nwarm,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 pair/3-body math, f64 accumulation", "data": "synthetic (seeded generator, teacher targets)",
+        "config": {"workload": f"batched minimal-Tersoff Si: {e.Nc} diamond configs of 8/64/216/512 atoms"
+                               if args.workload == 2 else data["name"],
+                   "population": P, "configs": e.Nc, "atoms": Natoms, "bonds": e.num_bonds,
+                   "units_per_step": P * Natoms, "l2": "flushed between steps (256 MiB write, outside the step events)",
+                   "parallelism": f"replicas{dist.world} (population per GPU, weak)"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": P * d * 4,
+                "d2h_bytes_per_step": P * 8 * 4, "latency_ms": {"p50": p50, "p99": p99}},
+        "gpu_launches": kernels_per_step * nsteps,
+        "roofline": roofline,
+        "plain_fp64": {"value": plain_value, "unit": UNIT, "individuals": npl,
+                       "speedup_batched_vs_plain_fp64": value / plain_value,
+                       "max_rel_fitness_err_vs_fp64": float(rel.max()), "ranking_identical": rank_same},
+        "clocks": clock_info,
+        "measured_peaks": {k: measured_peaks().get(k) for k in ("hbm_gbs", "bf16_tflops", "sm_max_mhz")},
+        "fitness_checksum": float(np.sum(fit_dev)),
+    }
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(data, args.cpu_seconds)
+    e.close()
+    return result
+
+
+def cpu_baseline(data, budget_s: float) -> dict:
+    """FP64 OpenMP oracle on the host cores over a bounded sample of the same population."""
+    from gpuga_b200 import synth
+    from oracle import oracle
+    oracle.build()
+    d = synth.write_dir(data, tempfile.mkdtemp(prefix="gpuga_cpu_"))
+    s = oracle.OracleSet(d)
+    pop = synth.population(data, 4096, seed=99)
+    t0 = time.perf_counter()
+    s.fitness(pop[:1])
+    t1 = time.perf_counter() - t0
+    n = int(max(1, min(len(pop), budget_s / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    s.fitness(pop[:n])
+    dt = time.perf_counter() - t0
+    s.close()
+    shutil.rmtree(d, ignore_errors=True)
+    return {"value": n * s.N / dt if False else n * int(data["Na"].sum()) / dt, "unit": UNIT,
+            "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"{n} individuals x full training set ({int(data['Na'].sum())} atoms), FP64 OpenMP oracle, "
+                      f"{dt:.1f} s"}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args, dist: Dist):
+    probe = os.path.join(ROOT, "oracle", "_ref", "ref_probe")
+    if dist.rank != 0:
+        return None
+    if not os.path.exists(probe):
+        return {"impl": "reference", "unavailable": "oracle/_ref/ref_probe was not built (needs the reference sources)"}
+    from gpuga_b200 import synth
+    data = synth.make(args.workload)
+    if args.workload == 4:
+        return {"impl": "reference", "unavailable": "the reference NN2B holds at most 10 neurons (nn2b.cuh:27-33)"}
+    data = synth.fill_targets(data, oracle_evaluator())
+    d = synth.write_dir(data, tempfile.mkdtemp(prefix="gpuga_ref_"))
+    P = int(data["ga"]["population_size"])
+    N = int(data["Na"].sum())
+    r = subprocess.run([probe, "time", d, str(P), str(args.steps), str(max(args.warmup, 3)), "12345678"],
+                       capture_output=True, text=True, timeout=3000)
+    shutil.rmtree(d, ignore_errors=True)
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("REF_TIME ")]
+    if r.returncode != 0 or not line:
+        return {"impl": "reference", "unavailable": f"ref_probe failed (rc={r.returncode}): {r.stderr[-300:]}"}
+    rt = json.loads(line[0][len("REF_TIME "):])
+    ms = rt["ms"]
+    value = P * N * len(ms) / (sum(ms) / 1e3)
+    sample = (f"reference CUDA build (GPUGA src/*.cu unmodified, nvcc -O3 --use_fast_math sm_100a) "
+              f"Fitness::compute, P={P}, {N} atoms, {len(ms)} generations on the GPU, wall time per generation")
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": len(ms),
+            "warmup": max(args.warmup, 3), "ms_per_step": sum(ms) / len(ms), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (fast-math)", "data": "synthetic",
+            "config": {"workload": "batched minimal-Tersoff Si" if args.workload == 2 else data["name"],
+                       "population": P, "atoms": N, "l2": "flushed between steps (256 MiB memset)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))}}
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return 0
+        res = run_reference(args, Dist.__new__(Dist) if False else _RankZero())
+        print(json.dumps(res))
+        return 0
+    dist = Dist()
+    try:
+        res = run_ours(args, dist)
+        if dist.rank == 0:
+            print(json.dumps(res))
+    finally:
+        dist.close()
+    return 0
+
+
+class _RankZero:
+    rank = 0
+    world = 1
+
+
+if __name__ == "__main__":
+    sys.exit(main())

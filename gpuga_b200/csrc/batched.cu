@@ -1,0 +1,825 @@
+// Batched fitness evaluation: every individual x every configuration of the
+// training set per generation.
+//
+// Decomposition.  A work item is (configuration c, group of G individuals).
+// Inside a CTA each warp lane is one individual (G = 32) or, for force
+// configurations whose per-bond force scratch would not fit in shared memory
+// for 32 individuals, G individuals x 32/G atoms.  With G = 32 a warp walks
+// one atom at a time for 32 parameter vectors: every geometry load is a
+// warp-uniform broadcast and the neighbor loops never diverge.  Per-lane
+// energy / virial / force-error sums stay in FP64 registers; a fixed-order
+// shared-memory reduction produces the (individual, configuration) results,
+// and a second kernel folds them into the weighted relative-RMSE fitness in a
+// fixed order, so a result never depends on what else shares the launch.
+//
+// Precision.  Pair, bond-order and three-body arithmetic is FP32 on CUDA cores
+// (accurate libdevice exp/pow/erfc/tanh, no fast-math); site energies and
+// virials are summed per atom in FP32 and across atoms in FP64; the loss and
+// normalisers are FP64.
+//
+// Geometry (unit vectors, distances, three-body cosines, RI Coulomb terms)
+// is parameter-independent and precomputed once (geometry.cu).
+#include <algorithm>
+#include <cmath>
+
+#include "engine.hpp"
+
+namespace gpuga {
+
+// ----------------------------------------------------------------- per-individual constants
+// Tersoff (minimal_tersoff.cu:39-75): per pair set s: lr = sqrt(2S)*A, la = sqrt(2/S)*A,
+// cr = D0/(S-1), ca = S*D0/(S-1), r0; then n, beta, h, R1, R2, pi/(R2-R1), -1/(2n).
+enum { TC_LR = 0, TC_LA = 2, TC_CR = 4, TC_CA = 6, TC_R0 = 8, TC_EN = 10, TC_BETA, TC_H, TC_R1, TC_R2, TC_PF,
+       TC_MHON, TC_COUNT };
+// RI (ri.cu:36-110): qq[3], a[3], b[3] = 1/rho, c[3], rc, v_rc, dv_rc, Morse lr, la, cr, ca, r0.
+enum { RC_QQ = 0, RC_A = 3, RC_B = 6, RC_C = 9, RC_RC = 12, RC_VRC, RC_DVRC, RC_LR, RC_LA, RC_CR, RC_CA, RC_R0,
+       RC_COUNT };
+
+int consts_per_individual(const DevSet& d) {
+  if (d.potential_type == 1 || d.potential_type == 2) return TC_COUNT;
+  if (d.potential_type == 0) return RC_COUNT;
+  return 1;
+}
+
+__device__ __forceinline__ float decode1(float mn, float mx, float x) {
+  return __fadd_rn(mn, __fmul_rn(__fsub_rn(mx, mn), x));  // fitness.cu:320-324, no contraction
+}
+
+// One thread per individual: FP32 decode exactly like the reference, derived
+// constants in FP64 rounded once to FP32.
+__global__ void decode_population(int P, int nv, int potential_type, int num_types, const float* __restrict__ pop,
+                                  const float* __restrict__ pmin, const float* __restrict__ pmax, int Pstride,
+                                  float* __restrict__ consts, float* __restrict__ weights) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const float* x = pop + (size_t)p * nv;
+  auto par = [&](int m) { return (double)decode1(pmin[m], pmax[m], x[m]); };
+  auto put = [&](int k, double v) { consts[(size_t)k * Pstride + p] = (float)v; };
+  if (potential_type == 1 || potential_type == 2) {
+    const int off = num_types == 2 ? 4 : 0;
+    for (int s = 0; s < 2; ++s) {
+      const int q = (num_types == 2 && s == 1) ? 4 : 0;
+      const double D0 = par(q + 0), A = par(q + 1), R0 = par(q + 2), S = par(q + 3);
+      put(TC_LR + s, sqrt(2.0 * S) * A);
+      put(TC_LA + s, sqrt(2.0 / S) * A);
+      put(TC_CR + s, D0 / (S - 1.0));
+      put(TC_CA + s, S * D0 / (S - 1.0));
+      put(TC_R0 + s, R0);
+    }
+    const double en = par(4 + off), R1 = par(7 + off), R2 = par(8 + off);
+    put(TC_EN, en);
+    put(TC_BETA, par(5 + off));
+    put(TC_H, par(6 + off));
+    put(TC_R1, R1);
+    put(TC_R2, R2);
+    put(TC_PF, M_PI / (R2 - R1));
+    put(TC_MHON, -0.5 / en);
+  } else if (potential_type == 0) {
+    const double q0 = par(0);
+    const double kc = 14.399645;  // ri.cu:29
+    put(RC_QQ + 0, q0 * q0 * kc);
+    put(RC_QQ + 1, -0.5 * q0 * q0 * kc);
+    put(RC_QQ + 2, 0.25 * q0 * q0 * kc);
+    for (int t = 0; t < 3; ++t) {
+      put(RC_A + t, par(1 + 3 * t));
+      put(RC_B + t, 1.0 / par(2 + 3 * t));
+      put(RC_C + t, par(3 + 3 * t));
+    }
+    const double rc = par(10), alpha = 0.2, pif = 0.225675833419103;
+    const double v_rc = erfc(alpha * rc) / rc;
+    const double dv_rc = -erfc(alpha * rc) / (rc * rc) - pif * exp(-alpha * alpha * rc * rc) / rc;
+    put(RC_RC, rc);
+    put(RC_VRC, v_rc);
+    put(RC_DVRC, dv_rc);
+    const double d0 = par(11), al = par(12), r0 = par(13), s = par(14);
+    put(RC_LR, sqrt(2.0 * s) * al);
+    put(RC_LA, sqrt(2.0 / s) * al);
+    put(RC_CR, d0 / (s - 1.0));
+    put(RC_CA, s * d0 / (s - 1.0));
+    put(RC_R0, r0);
+  } else {
+    for (int m = 0; m < nv; ++m) weights[(size_t)m * Pstride + p] = decode1(pmin[m], pmax[m], x[m]);
+  }
+}
+
+struct Consts {
+  const float* base;
+  int stride;
+  int p;
+  __device__ __forceinline__ float operator[](int k) const { return __ldg(base + (size_t)k * stride + p); }
+};
+
+// --------------------------------------------------------------------------- Tersoff
+struct TersoffC {
+  float lr[2], la[2], cr[2], ca[2], r0[2];
+  float en, beta, h, r1, r2, pf, mhon;
+};
+
+__device__ __forceinline__ void load_tersoff(const Consts& k, TersoffC& C) {
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    C.lr[s] = k[TC_LR + s];
+    C.la[s] = k[TC_LA + s];
+    C.cr[s] = k[TC_CR + s];
+    C.ca[s] = k[TC_CA + s];
+    C.r0[s] = k[TC_R0 + s];
+  }
+  C.en = k[TC_EN];
+  C.beta = k[TC_BETA];
+  C.h = k[TC_H];
+  C.r1 = k[TC_R1];
+  C.r2 = k[TC_R2];
+  C.pf = k[TC_PF];
+  C.mhon = k[TC_MHON];
+}
+
+// cutoff function of minimal_tersoff.cu:77-90
+__device__ __forceinline__ void cutoff_fn(float r1, float r2, float pf, float d, float& fc, float& fcp) {
+  if (d < r1) {
+    fc = 1.0f;
+    fcp = 0.0f;
+  } else if (d < r2) {
+    float s, c;
+    sincosf(pf * (d - r1), &s, &c);
+    fc = 0.5f * c + 0.5f;
+    fcp = -0.5f * pf * s;
+  } else {
+    fc = 0.0f;
+    fcp = 0.0f;
+  }
+}
+
+struct DevView {
+  int Nc, N, N_force;
+  const int* Na;
+  const int* Na_sum;
+  const int* NN;
+  const int* off;
+  const int* half_off;
+  const int* trip_off;
+  const int* rev;
+  const uint8_t* ptype;
+  const float4* g32;
+  const float4* gri;
+  const float* cosm;
+  const float* force_ref;
+};
+
+// Block-wide fixed-order reduction of the per-lane accumulators into res[p][c][k].
+__device__ __forceinline__ void reduce_item(const WorkItem& it, int P, int Nc, double (&acc)[kResK],
+                                            unsigned char* smem, double* __restrict__ res) {
+  __syncthreads();
+  double* red = reinterpret_cast<double*>(smem);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kResK; ++k) red[(warp * 32 + lane) * kResK + k] = acc[k];
+  __syncthreads();
+  const int G = it.G, A = 32 / G;
+  for (int t = threadIdx.x; t < G * kResK; t += blockDim.x) {
+    const int gg = t % G, k = t / G;
+    double s = 0.0;
+    for (int w = 0; w < kWarps; ++w)
+      for (int a = 0; a < A; ++a) s += red[(w * 32 + a * G + gg) * kResK + k];
+    const int p = it.p0 + gg;
+    if (p < P) res[((size_t)p * Nc + it.config) * kResK + k] = s;
+  }
+}
+
+// One atom of the minimal Tersoff potential (minimal_tersoff.cu:122-405) for
+// the lane's parameter vector.  Returns the site energy; writes the partial
+// forces f_ij (FORCE) or adds -r_ij (x) f_ij into v[6] (energy/virial items).
+//
+// With unit vectors u and the bond scalars
+//   S_k = b'_k fa_k, T_k = S_k fc_k, A'_j = fc'_j (fr_j - b_j fa_j) + fc_j (fr'_j - b_j fa'_j)
+// the reference's f_ij (minimal_tersoff.cu:250-307) is
+//   f_ij = 1/2 [ (A'_j - fc'_j sum_k T_k g_jk - m_j sum_k q_jk cos_jk) u_j + m_j sum_k q_jk u_k ]
+// with q_jk = beta (cos_jk - h) (S_j fc_k + T_k) and m_j = -2 fc_j / d_j.
+template <int ZC, bool FORCE>
+__device__ __forceinline__ float tersoff_atom(const DevView& S, const TersoffC& C, int i, int Z, float* fsm,
+                                              int bond0, int G, int g, float (&v)[6]) {
+  const int b0 = S.off[i];
+  float ux[ZC], uy[ZC], uz[ZC], dd[ZC];
+  int st[ZC];
+#pragma unroll
+  for (int j = 0; j < ZC; ++j) {
+    if (j < Z) {
+      const float4 q = __ldg(&S.g32[b0 + j]);
+      ux[j] = q.x;
+      uy[j] = q.y;
+      uz[j] = q.z;
+      dd[j] = q.w;
+      st[j] = S.ptype[b0 + j];
+    } else {
+      ux[j] = uy[j] = uz[j] = 0.f;
+      dd[j] = 1.0f;
+      st[j] = 0;
+    }
+  }
+  float fc[ZC], fcp[ZC], fr[ZC], fa[ZC], fcb[ZC];
+#pragma unroll
+  for (int j = 0; j < ZC; ++j) {
+    fc[j] = fcp[j] = fr[j] = fa[j] = fcb[j] = 0.f;
+    if (j < Z) {
+      const int s = st[j];
+      const float t = dd[j] - (s ? C.r0[1] : C.r0[0]);
+      fr[j] = (s ? C.cr[1] : C.cr[0]) * expf(-(s ? C.lr[1] : C.lr[0]) * t);
+      fa[j] = (s ? C.ca[1] : C.ca[0]) * expf(-(s ? C.la[1] : C.la[0]) * t);
+      cutoff_fn(C.r1, C.r2, C.pf, dd[j], fc[j], fcp[j]);
+      fcb[j] = fc[j] * C.beta;
+    }
+  }
+  const float* cs = S.cosm + S.trip_off[i];
+  float bb[ZC], Sb[ZC], Tb[ZC];
+#pragma unroll
+  for (int j = 0; j < ZC; ++j) {
+    bb[j] = 1.f;
+    Sb[j] = Tb[j] = 0.f;
+    if (j < Z) {
+      float zeta = 0.f;
+#pragma unroll
+      for (int k = 0; k < ZC; ++k) {
+        if (k < Z && k != j) {
+          const float x = __ldg(cs + j * Z + k) - C.h;
+          zeta = fmaf(fcb[k], x * x, zeta);
+        }
+      }
+      float b = 1.f, bp = 0.f;
+      if (!(zeta < 1.0e-16f)) {  // minimal_tersoff.cu:178-185
+        const float zn = powf(zeta, C.en);
+        const float opz = 1.0f + zn;
+        b = powf(opz, C.mhon);
+        bp = -0.5f * b * zn / (opz * zeta);
+      }
+      bb[j] = b;
+      Sb[j] = bp * fa[j];
+      Tb[j] = Sb[j] * fc[j];
+    }
+  }
+  float pe = 0.f;
+#pragma unroll
+  for (int j = 0; j < ZC; ++j) {
+    if (j < Z) {
+      const int s = st[j];
+      const float e = fr[j] - bb[j] * fa[j];
+      pe = fmaf(0.5f * fc[j], e, pe);
+      const float frp = -(s ? C.lr[1] : C.lr[0]) * fr[j];
+      const float fap = -(s ? C.la[1] : C.la[0]) * fa[j];
+      const float Ap = fcp[j] * e + fc[j] * (frp - bb[j] * fap);
+      float sumG = 0.f, accC = 0.f, Vx = 0.f, Vy = 0.f, Vz = 0.f;
+      const float Sj = Sb[j];
+#pragma unroll
+      for (int k = 0; k < ZC; ++k) {
+        if (k < Z && k != j) {
+          const float cjk = __ldg(cs + j * Z + k);
+          const float bx = C.beta * (cjk - C.h);
+          const float g = bx * (cjk - C.h);
+          const float q = bx * fmaf(Sj, fc[k], Tb[k]);
+          sumG = fmaf(Tb[k], g, sumG);
+          accC = fmaf(q, cjk, accC);
+          Vx = fmaf(q, ux[k], Vx);
+          Vy = fmaf(q, uy[k], Vy);
+          Vz = fmaf(q, uz[k], Vz);
+        }
+      }
+      const float m = -2.0f * fc[j] / dd[j];
+      const float cu = 0.5f * (Ap - fcp[j] * sumG - m * accC);
+      const float cv = 0.5f * m;
+      const float fx = fmaf(cu, ux[j], cv * Vx);
+      const float fy = fmaf(cu, uy[j], cv * Vy);
+      const float fz = fmaf(cu, uz[j], cv * Vz);
+      if (FORCE) {
+        const int bl = b0 + j - bond0;
+        fsm[(bl * 3 + 0) * G + g] = fx;
+        fsm[(bl * 3 + 1) * G + g] = fy;
+        fsm[(bl * 3 + 2) * G + g] = fz;
+      } else {
+        const float rx = dd[j] * ux[j], ry = dd[j] * uy[j], rz = dd[j] * uz[j];
+        v[0] = fmaf(-rx, fx, v[0]);
+        v[1] = fmaf(-ry, fy, v[1]);
+        v[2] = fmaf(-rz, fz, v[2]);
+        v[3] = fmaf(-rx, fy, v[3]);
+        v[4] = fmaf(-ry, fz, v[4]);
+        v[5] = fmaf(-rz, fx, v[5]);
+      }
+    }
+  }
+  return pe;
+}
+
+template <int ZC, bool FORCE>
+__global__ void __launch_bounds__(kBlock) tersoff_batched(DevView S, const WorkItem* __restrict__ items,
+                                                          const float* __restrict__ consts, int Pstride, int P,
+                                                          double* __restrict__ res, float* __restrict__ fdump) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const WorkItem it = items[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int G = it.G, A = 32 / G;
+  const int g = lane & (G - 1), aslot = lane / G;
+  const int p = it.p0 + g;
+  const Consts kc{consts, Pstride, p < P ? p : it.p0};
+  TersoffC C;
+  load_tersoff(kc, C);
+  const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
+  const int bond0 = S.off[atom0];
+  float* fsm = reinterpret_cast<float*>(smem);
+  double acc[kResK];
+#pragma unroll
+  for (int k = 0; k < kResK; ++k) acc[k] = 0.0;
+
+  for (int base = warp * A; base < Na; base += kWarps * A) {
+    const int il = base + aslot;
+    if (il < Na) {
+      const int i = atom0 + il;
+      float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      const float pe = tersoff_atom<ZC, FORCE>(S, C, i, S.NN[i], fsm, bond0, G, g, v);
+      if (!FORCE) {
+        acc[0] += (double)pe;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[1 + k] += (double)v[k];
+      }
+    }
+  }
+  if (FORCE) {
+    __syncthreads();
+    const int N = S.N, Nf = S.N_force;
+    for (int base = warp * A; base < Na; base += kWarps * A) {
+      const int il = base + aslot;
+      if (il < Na) {
+        const int i = atom0 + il;
+        const int b0 = S.off[i], Z = S.NN[i];
+        float Fx = 0.f, Fy = 0.f, Fz = 0.f;
+        for (int j = 0; j < Z; ++j) {
+          const int bl = b0 + j - bond0, rl = S.rev[b0 + j] - bond0;
+          Fx += fsm[(bl * 3 + 0) * G + g] - fsm[(rl * 3 + 0) * G + g];
+          Fy += fsm[(bl * 3 + 1) * G + g] - fsm[(rl * 3 + 1) * G + g];
+          Fz += fsm[(bl * 3 + 2) * G + g] - fsm[(rl * 3 + 2) * G + g];
+        }
+        const double dx = (double)Fx - (double)S.force_ref[i];
+        const double dy = (double)Fy - (double)S.force_ref[i + N];
+        const double dz = (double)Fz - (double)S.force_ref[i + 2 * (size_t)N];
+        acc[7] += dx * dx + dy * dy + dz * dz;
+        if (fdump && p < P) {
+          fdump[((size_t)p * 3 + 0) * Nf + i] = Fx;
+          fdump[((size_t)p * 3 + 1) * Nf + i] = Fy;
+          fdump[((size_t)p * 3 + 2) * Nf + i] = Fz;
+        }
+      }
+    }
+  }
+  reduce_item(it, P, S.Nc, acc, smem, res);
+}
+
+// --------------------------------------------------------------------------- RI / NN2B
+// RI pair term (ri.cu:77-110) with the geometry-only Coulomb pieces precomputed:
+// gri = (1/d, 1/d^6, erfc(alpha d)/d, erfc(alpha d)/d^2 + 2 alpha/sqrt(pi) exp(-alpha^2 d^2)/d).
+// Returns U(d) in p2 and dU/dd in fd.
+__device__ __forceinline__ void ri_pair(const Consts& k, int t, float d, float4 w, float& p2, float& fd) {
+  const float a = k[RC_A + t], b = k[RC_B + t], c = k[RC_C + t], qq = k[RC_QQ + t];
+  const float rc = k[RC_RC], vrc = k[RC_VRC], dvrc = k[RC_DVRC];
+  const float ex = expf(-d * b);
+  p2 = a * ex - c * w.y + qq * (w.z - vrc - dvrc * (d - rc));
+  fd = 6.0f * c * w.y * w.x - a * ex * b - qq * (w.w + dvrc);
+  if (t == 1) {
+    const float lr = k[RC_LR], la = k[RC_LA], dr = d - k[RC_R0];
+    const float fr = k[RC_CR] * expf(-lr * dr);
+    const float fa = k[RC_CA] * expf(-la * dr);
+    p2 += fr - fa;
+    fd += -lr * fr + la * fa;
+  }
+}
+
+// NN2B value and derivative (nn2b.cu:49-78) with the lane's weights in shared memory,
+// laid out [parameter][32 lanes].
+template <int NMAX>
+__device__ __forceinline__ void nn_pair(const float* __restrict__ wl, int n, float d, float& p2, float& f2) {
+  float x1[NMAX], y1[NMAX];
+#pragma unroll
+  for (int a = 0; a < NMAX; ++a) {
+    x1[a] = y1[a] = 0.f;
+    if (a < n) {
+      const float w0 = wl[a * 32];
+      x1[a] = tanhf(w0 * d - wl[(a + n) * 32]);
+      y1[a] = (1.0f - x1[a] * x1[a]) * w0;
+    }
+  }
+  p2 = 0.f;
+  f2 = 0.f;
+  for (int a = 0; a < n; ++a) {
+    const float* w1 = wl + (2 * n + a * n) * 32;
+    float x2 = 0.f, y2 = 0.f;
+#pragma unroll
+    for (int m = 0; m < NMAX; ++m) {
+      if (m < n) {
+        const float w = w1[m * 32];
+        x2 = fmaf(w, x1[m], x2);
+        y2 = fmaf(w, y1[m], y2);
+      }
+    }
+    x2 = tanhf(x2 - wl[(n * (n + 2) + a) * 32]);
+    y2 *= 1.0f - x2 * x2;
+    const float w2 = wl[(n * (n + 3) + a) * 32];
+    p2 = fmaf(w2, x2, p2);
+    f2 = fmaf(w2, y2, f2);
+  }
+  p2 -= wl[(n * (n + 4)) * 32];
+}
+
+struct NNTaper {
+  float r1, r2, pf;
+  int consistent;
+};
+
+template <int KIND, int NMAX, bool FORCE>
+__global__ void __launch_bounds__(kBlock) pair_batched(DevView S, const WorkItem* __restrict__ items,
+                                                       const float* __restrict__ consts,
+                                                       const float* __restrict__ weights, int Pstride, int P,
+                                                       int nn, int nv, NNTaper tp, double* __restrict__ res) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const WorkItem it = items[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int p = it.p0 + lane;
+  const int pl = p < P ? p : it.p0;
+  const Consts kc{consts, Pstride, pl};
+  float* wsm = reinterpret_cast<float*>(smem + (size_t)kWarps * 32 * kResK * sizeof(double));
+  if (KIND == 2) {
+    for (int t = threadIdx.x; t < nv * 32; t += blockDim.x) {
+      const int m = t >> 5, l = t & 31;
+      const int pp = it.p0 + l < P ? it.p0 + l : it.p0;
+      wsm[t] = weights[(size_t)m * Pstride + pp];
+    }
+    __syncthreads();
+  }
+  const float* wl = wsm + lane;
+  const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
+  const int N = S.N;
+  double acc[kResK];
+#pragma unroll
+  for (int k = 0; k < kResK; ++k) acc[k] = 0.0;
+  for (int il = warp; il < Na; il += kWarps) {
+    const int i = atom0 + il;
+    const int bbeg = FORCE ? S.off[i] : S.half_off[i];
+    const int bend = S.off[i + 1];
+    double Fx = 0, Fy = 0, Fz = 0;
+    for (int b = bbeg; b < bend; ++b) {
+      const float4 q = __ldg(&S.g32[b]);
+      const float d = q.w;
+      float p2, fd;
+      if (KIND == 1) {
+        ri_pair(kc, S.ptype[b], d, __ldg(&S.gri[b]), p2, fd);
+      } else {
+        float f2raw;
+        nn_pair<NMAX>(wl, nn, d, p2, f2raw);
+        float fc, fcp;
+        cutoff_fn(tp.r1, tp.r2, tp.pf, d, fc, fcp);
+        if (tp.consistent) {
+          fd = f2raw * fc + p2 * fcp;
+          p2 *= fc;
+        } else {  // nn2b.cu:147-148: p2 is tapered before it enters the force
+          p2 *= fc;
+          fd = f2raw * fc + p2 * fcp;
+        }
+      }
+      if (FORCE) {
+        Fx = fma((double)fd, (double)q.x, Fx);
+        Fy = fma((double)fd, (double)q.y, Fy);
+        Fz = fma((double)fd, (double)q.z, Fz);
+      } else {
+        // unordered pair: full U and -r (x) r f2 with f2 = fd / d, i.e. -d fd u (x) u
+        acc[0] += (double)p2;
+        const float s = d * fd;
+        const float sx = s * q.x, sy = s * q.y, sz = s * q.z;
+        acc[1] = fma(-(double)sx, (double)q.x, acc[1]);
+        acc[2] = fma(-(double)sy, (double)q.y, acc[2]);
+        acc[3] = fma(-(double)sz, (double)q.z, acc[3]);
+        acc[4] = fma(-(double)sx, (double)q.y, acc[4]);
+        acc[5] = fma(-(double)sy, (double)q.z, acc[5]);
+        acc[6] = fma(-(double)sz, (double)q.x, acc[6]);
+      }
+    }
+    if (FORCE) {
+      const double dx = Fx - (double)S.force_ref[i];
+      const double dy = Fy - (double)S.force_ref[i + N];
+      const double dz = Fz - (double)S.force_ref[i + 2 * (size_t)N];
+      acc[7] += dx * dx + dy * dy + dz * dz;
+    }
+  }
+  reduce_item(it, P, S.Nc, acc, smem, res);
+}
+
+// --------------------------------------------------------------------------- fitness
+// fitness.cu:329-331, 437-555 in FP64: one warp per individual, fixed-order sums.
+__global__ void fitness_reduce(int P, int Nc, int Nc_force, const double* __restrict__ res,
+                               const double* __restrict__ E_ref, const double* __restrict__ W_ref, double nF,
+                               double nE, double nW, float wF, float wE, float wW, double* __restrict__ fitness,
+                               double* __restrict__ comps) {
+  const int p = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (p >= P) return;
+  double eE = 0, eW = 0, eF = 0;
+  for (int c = lane; c < Nc; c += 32) {
+    const double* r = res + ((size_t)p * Nc + c) * kResK;
+    if (c >= Nc_force) {
+      const double de = r[0] - E_ref[c];
+      eE += de * de;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double dw = r[1 + k] - W_ref[c + (size_t)Nc * k];
+        eW += dw * dw;
+      }
+    } else {
+      eF += r[7];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    eE += __shfl_xor_sync(0xffffffffu, eE, o);
+    eW += __shfl_xor_sync(0xffffffffu, eW, o);
+    eF += __shfl_xor_sync(0xffffffffu, eF, o);
+  }
+  if (lane == 0) {
+    const double rE = sqrt(eE / nE), rW = sqrt(eW / nW), rF = sqrt(eF / nF);
+    fitness[p] = (double)wE * rE + (double)wW * rW + (double)wF * rF;
+    if (comps) {
+      comps[3 * (size_t)p + 0] = rE;
+      comps[3 * (size_t)p + 1] = rW;
+      comps[3 * (size_t)p + 2] = rF;
+    }
+  }
+}
+
+// --------------------------------------------------------------------------- planning
+namespace {
+constexpr size_t kRedBytes = (size_t)kWarps * 32 * kResK * sizeof(double);
+constexpr size_t kForceSmemTarget = 96 * 1024;  // two CTAs per SM
+constexpr size_t kSmemMax = 220 * 1024;
+
+int zclass_of(int z) { return z <= 4 ? 4 : (z <= 8 ? 8 : (z <= 16 ? 16 : 0)); }
+int nmax_of(int n) { return n <= 8 ? 8 : (n <= 16 ? 16 : (n <= 32 ? 32 : 0)); }
+}  // namespace
+
+DevView make_view(const DevSet& d) {
+  DevView v;
+  v.Nc = d.Nc;
+  v.N = d.N;
+  v.N_force = d.N_force;
+  v.Na = d.Na;
+  v.Na_sum = d.Na_sum;
+  v.NN = d.NN;
+  v.off = d.off;
+  v.half_off = d.half_off;
+  v.trip_off = d.trip_off;
+  v.rev = d.rev;
+  v.ptype = d.ptype;
+  v.g32 = d.g32;
+  v.gri = d.gri;
+  v.cosm = d.cosm;
+  v.force_ref = d.force_ref;
+  return v;
+}
+
+static int launch_one(Engine* e, Plan* plan, const Launch& L, cudaStream_t st, bool configure_only);
+
+int plan_build(Engine* e, int P, Plan** out) {
+  const DevSet& d = e->d;
+  const TrainingSet& ts = e->ts;
+  std::unique_ptr<Plan> plan(new Plan);
+  plan->P = P;
+  plan->Pstride = (P + 31) & ~31;
+  const bool tersoff = d.potential_type == 1 || d.potential_type == 2;
+  const int kind = tersoff ? 0 : (d.potential_type == 0 ? 1 : 2);
+  if (kind == 2 && nmax_of(d.num_neurons) == 0) {
+    set_error("batched NN2B supports up to 32 neurons per layer (got %d).", d.num_neurons);
+    return GPUGA_ERR_UNSUPPORTED;
+  }
+  struct Tmp {
+    WorkItem w;
+    double cost, units, flops, sfu;
+  };
+  // Algorithmic work per (individual, atom), counted on the batched formulation
+  // (FMA = 2 flops; exp/pow/erfc/tanh/sin-cos calls counted as SFU work):
+  //   Tersoff: 60 flops + 4 transcendentals per bond, 21 flops per ordered triplet
+  //   RI:      20 flops + 1 exp per pair (+10 flops + 2 exp for cation-anion Morse)
+  //   NN2B:    4n^2 + 13n + 10 flops + 2n tanh per pair
+  std::vector<double> atom_flops(ts.N), atom_sfu(ts.N), atom_flops_half(ts.N), atom_sfu_half(ts.N);
+  for (int i = 0; i < ts.N; ++i) {
+    const double Z = e->h_NN[i];
+    if (kind == 0) {
+      atom_flops[i] = 60.0 * Z + 21.0 * Z * (Z - 1.0);
+      atom_sfu[i] = 4.0 * Z;
+    } else {
+      const double nn = d.num_neurons;
+      const double fpp = kind == 1 ? 25.0 : 4.0 * nn * nn + 13.0 * nn + 10.0;
+      const double spp = kind == 1 ? 2.0 : 2.0 * nn;
+      int half = 0;
+      for (int b = e->h_off[i]; b < e->h_off[i + 1]; ++b) half += e->h_nbr[b] > i;
+      atom_flops[i] = fpp * Z;
+      atom_sfu[i] = spp * Z;
+      atom_flops_half[i] = fpp * half;
+      atom_sfu_half[i] = spp * half;
+    }
+  }
+  std::map<std::pair<int, int>, std::vector<Tmp>> groups;  // (zclass, force) -> items
+  std::map<std::pair<int, int>, size_t> smem_need;
+  for (int c = 0; c < ts.Nc; ++c) {
+    const bool force = c < ts.Nc_force;
+    const int Na = ts.Na[c];
+    const long long Bc = (long long)e->h_off[ts.Na_sum[c] + Na] - e->h_off[ts.Na_sum[c]];
+    int zc = 0, G = 32;
+    size_t smem = kRedBytes;
+    double per_atom;
+    if (kind == 0) {
+      zc = zclass_of(e->h_zmax[c]);
+      if (zc == 0) {
+        set_error("configuration %d has an atom with %d neighbors; the batched Tersoff path supports 16.", c,
+                  e->h_zmax[c]);
+        return GPUGA_ERR_UNSUPPORTED;
+      }
+      if (force) {
+        const size_t per_ind = (size_t)Bc * 3 * sizeof(float);
+        while (G > 1 && per_ind * G > kForceSmemTarget) G >>= 1;
+        if (per_ind * G > kSmemMax) {
+          set_error("configuration %d needs %zu bytes of force scratch per individual.", c, per_ind);
+          return GPUGA_ERR_UNSUPPORTED;
+        }
+        smem = std::max(smem, per_ind * G);
+      }
+      per_atom = (double)zc * zc + 8.0 * zc;
+    } else {
+      if (kind == 2) smem += (size_t)d.num_vars * 32 * sizeof(float);
+      per_atom = (double)Bc / Na * (force ? 1.0 : 0.5) * (kind == 2 ? 4.0 * d.num_neurons * d.num_neurons : 40.0);
+    }
+    auto key = std::make_pair(zc, force ? 1 : 0);
+    smem_need[key] = std::max(smem_need[key], smem);
+    double cf = 0, cs = 0;
+    const bool half = kind != 0 && !force;
+    for (int k = 0; k < Na; ++k) {
+      const int i = ts.Na_sum[c] + k;
+      cf += half ? atom_flops_half[i] : atom_flops[i];
+      cs += half ? atom_sfu_half[i] : atom_sfu[i];
+    }
+    for (int p0 = 0; p0 < P; p0 += G) {
+      const int cnt = std::min(G, P - p0);
+      groups[key].push_back({WorkItem{c, p0, G, force ? 1 : 0}, per_atom * Na * cnt, (double)Na * cnt, cf * cnt,
+                             cs * cnt});
+    }
+  }
+  size_t total = 0;
+  for (auto& kv : groups) total += kv.second.size();
+  GPUGA_TRY(e->alloc(&plan->d_items, std::max<size_t>(total, 1)));
+  std::vector<WorkItem> all;
+  all.reserve(total);
+  for (auto& kv : groups) {
+    auto& v = kv.second;
+    std::stable_sort(v.begin(), v.end(), [](const Tmp& a, const Tmp& b) { return a.cost > b.cost; });
+    Launch L;
+    L.kind = kind;
+    L.zclass = kv.first.first;
+    L.force = kv.first.second != 0;
+    L.smem = smem_need[kv.first];
+    L.count = (int)v.size();
+    L.d_items = plan->d_items + all.size();
+    for (auto& t : v) {
+      all.push_back(t.w);
+      L.units += t.units;
+      L.flops += t.flops;
+      L.sfu += t.sfu;
+    }
+    plan->launches.push_back(L);
+  }
+  // largest launches first so the side stream gets the long ones early
+  std::stable_sort(plan->launches.begin(), plan->launches.end(),
+                   [](const Launch& a, const Launch& b) { return a.count > b.count; });
+  GPUGA_CUDA(cudaMemcpy(plan->d_items, all.data(), sizeof(WorkItem) * all.size(), cudaMemcpyHostToDevice));
+  const int K = consts_per_individual(d);
+  GPUGA_TRY(e->alloc(&plan->d_consts, (size_t)K * plan->Pstride));
+  if (kind == 2) GPUGA_TRY(e->alloc(&plan->d_weights, (size_t)d.num_vars * plan->Pstride));
+  GPUGA_TRY(e->alloc(&plan->d_res, (size_t)P * d.Nc * kResK));
+  GPUGA_TRY(e->alloc(&plan->d_fitness, (size_t)P));
+  GPUGA_TRY(e->alloc(&plan->d_comps, (size_t)3 * P));
+  GPUGA_TRY(e->alloc(&plan->d_pop, (size_t)P * d.num_vars));
+  GPUGA_CUDA(cudaMallocHost(&plan->h_pop, sizeof(float) * (size_t)P * d.num_vars));
+  GPUGA_CUDA(cudaMallocHost(&plan->h_fit, sizeof(double) * 4 * (size_t)P));
+  GPUGA_CUDA(cudaStreamCreateWithFlags(&plan->side, cudaStreamNonBlocking));
+  GPUGA_CUDA(cudaEventCreateWithFlags(&plan->fork, cudaEventDisableTiming));
+  GPUGA_CUDA(cudaEventCreateWithFlags(&plan->join, cudaEventDisableTiming));
+  plan->tev.assign(2 * plan->launches.size(), nullptr);
+  for (auto& ev : plan->tev) GPUGA_CUDA(cudaEventCreate(&ev));
+  plan->t_ms.assign(plan->launches.size(), 0.0);
+  for (const Launch& L : plan->launches) GPUGA_TRY(launch_one(e, plan.get(), L, nullptr, true));
+  *out = plan.release();
+  return GPUGA_OK;
+}
+
+template <class K>
+static int set_smem(K kernel, size_t smem) {
+  GPUGA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(smem, kSmemMax)));
+  return GPUGA_OK;
+}
+
+// configure_only: set the dynamic shared-memory limit of the launch's kernel
+// (done once when the plan is built, never inside a stream capture).
+static int launch_one(Engine* e, Plan* plan, const Launch& L, cudaStream_t st, bool configure_only) {
+  const DevSet& d = e->d;
+  const DevView v = make_view(d);
+  const int P = plan->P;
+  const dim3 grid(L.count), block(kBlock);
+#define GPUGA_TERSOFF(ZC, F)                                                                           \
+  do {                                                                                                 \
+    if (configure_only) {                                                                              \
+      GPUGA_TRY(set_smem(tersoff_batched<ZC, F>, L.smem));                                             \
+      break;                                                                                           \
+    }                                                                                                  \
+    tersoff_batched<ZC, F><<<grid, block, L.smem, st>>>(v, L.d_items, plan->d_consts, plan->Pstride, P, \
+                                                        plan->d_res, plan->dump ? plan->d_fdump : nullptr);                  \
+  } while (0)
+  if (L.kind == 0) {
+    if (L.zclass == 4) {
+      if (L.force) GPUGA_TERSOFF(4, true); else GPUGA_TERSOFF(4, false);
+    } else if (L.zclass == 8) {
+      if (L.force) GPUGA_TERSOFF(8, true); else GPUGA_TERSOFF(8, false);
+    } else {
+      if (L.force) GPUGA_TERSOFF(16, true); else GPUGA_TERSOFF(16, false);
+    }
+  } else {
+    NNTaper tp{e->spec.nn_r1, e->spec.nn_r2, (float)(M_PI / ((double)e->spec.nn_r2 - e->spec.nn_r1)),
+               e->spec.nn_consistent};
+#define GPUGA_PAIR(KD, NM, F)                                                                           \
+  do {                                                                                                  \
+    if (configure_only) {                                                                               \
+      GPUGA_TRY(set_smem(pair_batched<KD, NM, F>, L.smem));                                             \
+      break;                                                                                            \
+    }                                                                                                   \
+    pair_batched<KD, NM, F><<<grid, block, L.smem, st>>>(v, L.d_items, plan->d_consts, plan->d_weights, \
+                                                         plan->Pstride, P, d.num_neurons, d.num_vars, tp,   \
+                                                         plan->d_res);                                  \
+  } while (0)
+    if (L.kind == 1) {
+      if (L.force) GPUGA_PAIR(1, 8, true); else GPUGA_PAIR(1, 8, false);
+    } else {
+      const int nm = nmax_of(d.num_neurons);
+      if (nm == 8) {
+        if (L.force) GPUGA_PAIR(2, 8, true); else GPUGA_PAIR(2, 8, false);
+      } else if (nm == 16) {
+        if (L.force) GPUGA_PAIR(2, 16, true); else GPUGA_PAIR(2, 16, false);
+      } else {
+        if (L.force) GPUGA_PAIR(2, 32, true); else GPUGA_PAIR(2, 32, false);
+      }
+    }
+  }
+#undef GPUGA_TERSOFF
+#undef GPUGA_PAIR
+  GPUGA_CUDA(cudaGetLastError());
+  return GPUGA_OK;
+}
+
+// Folds the event pairs of the previous timed generation into the per-launch totals.
+int plan_collect_timing(Plan* plan) {
+  if (!plan->t_pending) return GPUGA_OK;
+  for (size_t k = 0; k < plan->launches.size(); ++k) {
+    GPUGA_CUDA(cudaEventSynchronize(plan->tev[2 * k + 1]));
+    float ms = 0.f;
+    GPUGA_CUDA(cudaEventElapsedTime(&ms, plan->tev[2 * k], plan->tev[2 * k + 1]));
+    plan->t_ms[k] += ms;
+  }
+  plan->t_count += 1;
+  plan->t_pending = false;
+  return GPUGA_OK;
+}
+
+// Enqueues one generation: decode, the batched force launches (energy/virial
+// items on `st`, force items on the plan's side stream), then the fitness fold.
+int batched_enqueue(Engine* e, Plan* plan, const float* d_pop, double* d_fitness, cudaStream_t st) {
+  const DevSet& d = e->d;
+  const int P = plan->P;
+  decode_population<<<(P + 127) / 128, 128, 0, st>>>(P, d.num_vars, d.potential_type, d.num_types, d_pop,
+                                                     e->d_pmin, e->d_pmax, plan->Pstride, plan->d_consts,
+                                                     plan->d_weights);
+  GPUGA_CUDA(cudaGetLastError());
+  bool any_side = false;
+  for (const Launch& L : plan->launches)
+    if (L.force) any_side = true;
+  if (any_side) {
+    GPUGA_CUDA(cudaEventRecord(plan->fork, st));
+    GPUGA_CUDA(cudaStreamWaitEvent(plan->side, plan->fork, 0));
+  }
+  GPUGA_TRY(plan_collect_timing(plan));
+  for (size_t k = 0; k < plan->launches.size(); ++k) {
+    const Launch& L = plan->launches[k];
+    cudaStream_t ls = L.force ? plan->side : st;
+    if (plan->timing) GPUGA_CUDA(cudaEventRecord(plan->tev[2 * k], ls));
+    GPUGA_TRY(launch_one(e, plan, L, ls, false));
+    if (plan->timing) GPUGA_CUDA(cudaEventRecord(plan->tev[2 * k + 1], ls));
+  }
+  plan->t_pending = plan->timing;
+  if (any_side) {
+    GPUGA_CUDA(cudaEventRecord(plan->join, plan->side));
+    GPUGA_CUDA(cudaStreamWaitEvent(st, plan->join, 0));
+  }
+  fitness_reduce<<<(P + 3) / 4, 128, 0, st>>>(P, d.Nc, d.Nc_force, plan->d_res, d.E_ref, d.W_ref, d.norm_force,
+                                              d.norm_energy, d.norm_virial, d.w_force, d.w_energy, d.w_stress,
+                                              d_fitness, plan->d_comps);
+  GPUGA_CUDA(cudaGetLastError());
+  return GPUGA_OK;
+}
+
+}  // namespace gpuga

@@ -1,0 +1,157 @@
+// Engine: one training set resident in HBM plus the buffers of the batched
+// fitness evaluation.  Layout (all device arrays):
+//
+//   configs  Na[Nc], Na_sum[Nc], cfg_zmax[Nc]
+//   atoms    type[N], r[3N] (SoA, FP32 as parsed), NN[N], off[N+1] (CSR into bonds),
+//            half_off[N] (first bond whose neighbor index is > i), trip_off[N+1]
+//   bonds    nbr[B], rev[B] (reverse bond), ptype[B] (pair set / RI pair type),
+//            g32[B] float4 (unit vector, d), g64[B] double4 (x,y,z,d),
+//            gri[B] float4 (RI geometry-only terms), image shift from the FP32 MIC
+//   triplets cosm[sum Z_i^2] FP32 cos(theta_ijk), row j col k of atom i's Z_i x Z_i block
+//   targets  force_ref[3N], E_ref[Nc], W_ref[6Nc] (FP64 copies of the FP32 inputs)
+//
+// Bond vectors use the periodic image chosen by the reference's FP32 rule and
+// are then evaluated in FP64 from the FP32 positions.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "common.hpp"
+
+namespace gpuga {
+
+constexpr int kBlock = 256;           // threads per CTA of the batched kernels
+constexpr int kWarps = kBlock / 32;
+constexpr int kResK = 8;              // per (individual, config): E, W[6], sum|dF|^2
+constexpr int kMaxConsts = 32;        // per-individual FP32 constants of the batched kernels
+
+struct DevSet {
+  int Nc = 0, Nc_force = 0, N = 0, N_force = 0, B = 0, max_Na = 0, max_Z = 0;
+  int potential_type = -1, num_types = 1, num_neurons = 0, num_vars = 0;
+  int* Na = nullptr;
+  int* Na_sum = nullptr;
+  int* type = nullptr;
+  float* r = nullptr;
+  float* h = nullptr;
+  int* NN = nullptr;
+  int* off = nullptr;
+  int* half_off = nullptr;
+  int* trip_off = nullptr;
+  int* nbr = nullptr;
+  int* rev = nullptr;
+  uint8_t* ptype = nullptr;
+  float4* g32 = nullptr;
+  double4* g64 = nullptr;
+  float4* gri = nullptr;
+  float* cosm = nullptr;
+  float* force_ref = nullptr;
+  double* E_ref = nullptr;
+  double* W_ref = nullptr;
+  double norm_force = 0, norm_energy = 0, norm_virial = 0;
+  float w_force = 0, w_energy = 0, w_stress = 0;
+};
+
+// One CTA of a batched launch: config c for individuals [p0, p0 + G).
+struct WorkItem {
+  int config;
+  int p0;
+  int G;      // individuals per item (power of two <= 32); lanes = G individuals x (32/G) atoms
+  int flags;  // bit0: force configuration
+};
+
+struct Launch {
+  int kind = 0;        // 0 Tersoff, 1 RI, 2 NN2B
+  double units = 0;    // (individual, atom) pairs per launch
+  double flops = 0;    // algorithmic FP32 flops per launch (FMA = 2)
+  double sfu = 0;      // transcendental calls per launch
+  int zclass = 4;      // Tersoff register-array size
+  bool force = false;  // force items (gather pass) vs energy/virial items
+  size_t smem = 0;
+  int count = 0;
+  WorkItem* d_items = nullptr;  // slice of the engine's item buffer
+};
+
+struct Plan {
+  int P = 0;
+  std::vector<Launch> launches;
+  WorkItem* d_items = nullptr;
+  float* d_consts = nullptr;   // [kMaxConsts][Pstride] per-individual constants
+  float* d_weights = nullptr;  // NN2B weights [num_vars][Pstride]
+  int Pstride = 0;
+  double* d_res = nullptr;     // [P][Nc][kResK]
+  double* d_fitness = nullptr; // [P]
+  double* d_comps = nullptr;   // [P][3]
+  float* d_pop = nullptr;      // [P][d] staging
+  float* h_pop = nullptr;      // pinned
+  double* h_fit = nullptr;     // pinned [4P]: fitness + 3 components
+  float* d_fdump = nullptr;    // optional per-atom forces of force configs [P][3][N_force]
+  bool dump = false;           // pass d_fdump to the kernels (eager launches only)
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t side = nullptr;
+  bool timing = false;                // record an event pair around every launch (eager launches)
+  std::vector<cudaEvent_t> tev;       // 2 per launch
+  std::vector<double> t_ms;           // accumulated device time per launch
+  int t_count = 0;                    // generations accumulated
+  bool t_pending = false;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+struct Engine {
+  gpuga_options opt{};
+  PotentialSpec spec;
+  TrainingSet ts;
+  DevSet d;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  float* d_pmin = nullptr;
+  float* d_pmax = nullptr;
+  std::vector<int> h_NN, h_off, h_nbr, h_zmax;  // host copies of the neighbor list
+  std::map<int, std::unique_ptr<Plan>> plans;    // keyed by population size
+  size_t device_bytes = 0;
+  std::vector<void*> allocations;
+  // plain-path scratch
+  double* s64 = nullptr;  // per-bond scratch (b, bp, fx, fy, fz) FP64
+  float* s32 = nullptr;
+  double* p64_F = nullptr;
+  double* p64_W = nullptr;
+  double* p64_pe = nullptr;
+  float* p32_F = nullptr;
+  float* p32_W = nullptr;
+  float* p32_pe = nullptr;
+  double* p_out = nullptr;  // per-individual fitness + components of the plain path [4P]
+  int p_out_cap = 0;
+  ~Engine();
+  int dalloc(void** p, size_t bytes);
+  template <class T>
+  int alloc(T** p, size_t n) {
+    return dalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+  }
+};
+
+// geometry.cu
+int build_geometry(Engine* e);
+// FP32 neighbor rule of neighbor.cu:30-66 on reference-layout device arrays.
+int neighbor_reference_layout(int Nc, int N, int max_Na, const int* Na, const int* Na_sum, const float* r,
+                              const float* h, float cutoff, int* NN, int* NL, cudaStream_t st);
+
+// batched.cu
+int plan_build(Engine* e, int P, Plan** out);
+int batched_enqueue(Engine* e, Plan* plan, const float* d_pop, double* d_fitness, cudaStream_t st);
+int consts_per_individual(const DevSet& d);
+int plan_collect_timing(Plan* plan);
+int plan_get(Engine* e, int P, Plan** out);
+
+// plain.cu
+int plain_fitness(Engine* e, bool fp64, int P, const float* pop01, double* fitness, double* comps);
+int plain_find_force64(Engine* e, const double* params, double* F, double* W, double* pe);
+int plain_find_force32(Engine* e, const float* params, float* F, float* W, float* pe);
+
+// engine.cu
+int engine_create(const PotentialSpec& spec, TrainingSet&& ts, const gpuga_options& opt, Engine** out);
+int engine_fitness(Engine* e, int path, int P, const float* pop01, double* fitness, double* comps);
+
+}  // namespace gpuga

@@ -1,0 +1,283 @@
+// Neighbor list and parameter-independent geometry.
+//
+// The list is built with the reference's FP32 rule (neighbor.cu:30-66,
+// mic.cuh:20-32): same-config atoms, ascending n2, strict d^2 < rc^2 in FP32,
+// nearest image by round-half-even of the fractional coordinates.  Every FP32
+// operation is an explicit round-to-nearest intrinsic so the compiler cannot
+// fuse differently from the pinned pattern (kMicMode).
+//
+// From the list the engine derives, once per training set, everything that
+// does not depend on the potential parameters: FP64 bond vectors for the
+// image the FP32 rule picked, unit vectors and distances in FP32, reverse-bond
+// indices, three-body cosines and the fixed-damping Coulomb terms of the RI
+// potential.
+#include <cmath>
+#include <numeric>
+
+#include "engine.hpp"
+
+namespace gpuga {
+
+// Contraction pattern of the three-term dot products in the FP32 MIC and the
+// squared distance; pinned against the reference build.
+//   0: fma(a2,b2, fma(a0,b0, a1*b1))   1: fma(a2,b2, fma(a1,b1, a0*b0))   2: no fusion
+#ifndef GPUGA_MIC_MODE
+#define GPUGA_MIC_MODE 0
+#endif
+constexpr int kMicMode = GPUGA_MIC_MODE;
+
+template <int MODE>
+__device__ __forceinline__ float dot3(float a0, float b0, float a1, float b1, float a2, float b2) {
+  if (MODE == 0) return __fmaf_rn(a2, b2, __fmaf_rn(a0, b0, __fmul_rn(a1, b1)));
+  if (MODE == 1) return __fmaf_rn(a2, b2, __fmaf_rn(a1, b1, __fmul_rn(a0, b0)));
+  return __fadd_rn(__fadd_rn(__fmul_rn(a0, b0), __fmul_rn(a1, b1)), __fmul_rn(a2, b2));
+}
+
+// mic.cuh:20-32; also returns the image shift that was removed.
+template <int MODE>
+__device__ __forceinline__ void mic32(const float* h, float& x, float& y, float& z, float& ix, float& iy,
+                                      float& iz) {
+  float sx = dot3<MODE>(h[9], x, h[10], y, h[11], z);
+  float sy = dot3<MODE>(h[12], x, h[13], y, h[14], z);
+  float sz = dot3<MODE>(h[15], x, h[16], y, h[17], z);
+  ix = rintf(sx);
+  iy = rintf(sy);
+  iz = rintf(sz);
+  sx = __fsub_rn(sx, ix);
+  sy = __fsub_rn(sy, iy);
+  sz = __fsub_rn(sz, iz);
+  x = dot3<MODE>(h[0], sx, h[1], sy, h[2], sz);
+  y = dot3<MODE>(h[3], sx, h[4], sy, h[5], sz);
+  z = dot3<MODE>(h[6], sx, h[7], sy, h[8], sz);
+}
+
+// One CTA per configuration, atoms strided over the threads.  Pass 0 counts,
+// pass 1 writes the CSR list and the image shifts.
+template <int MODE, bool FILL>
+__global__ void neighbor_scan(int N, const int* __restrict__ Na, const int* __restrict__ Na_sum,
+                              float rc2, const float* __restrict__ box, const float* __restrict__ r,
+                              int* __restrict__ NN, const int* __restrict__ off, int* __restrict__ nbr,
+                              float* __restrict__ img) {
+  const int c = blockIdx.x;
+  const int n_begin = Na_sum[c], n_end = n_begin + Na[c];
+  const float* h = box + 18 * (size_t)c;
+  float hh[18];
+#pragma unroll
+  for (int k = 0; k < 18; ++k) hh[k] = h[k];
+  for (int n1 = n_begin + threadIdx.x; n1 < n_end; n1 += blockDim.x) {
+    const float x1 = r[n1], y1 = r[n1 + N], z1 = r[n1 + 2 * (size_t)N];
+    int count = 0;
+    int base = FILL ? off[n1] : 0;
+    for (int n2 = n_begin; n2 < n_end; ++n2) {
+      if (n2 == n1) continue;
+      float x12 = __fsub_rn(r[n2], x1);
+      float y12 = __fsub_rn(r[n2 + N], y1);
+      float z12 = __fsub_rn(r[n2 + 2 * (size_t)N], z1);
+      float ix, iy, iz;
+      mic32<MODE>(hh, x12, y12, z12, ix, iy, iz);
+      const float d2 = dot3<MODE>(x12, x12, y12, y12, z12, z12);
+      if (d2 < rc2) {
+        if (FILL) {
+          nbr[base + count] = n2;
+          img[3 * (size_t)(base + count) + 0] = ix;
+          img[3 * (size_t)(base + count) + 1] = iy;
+          img[3 * (size_t)(base + count) + 2] = iz;
+        }
+        ++count;
+      }
+    }
+    if (!FILL) NN[n1] = count;
+  }
+}
+
+// Reference layout NL[k*N + n1] (neighbor.cu:61) for the drop-in entry point.
+template <int MODE>
+__global__ void neighbor_reference(int N, const int* __restrict__ Na, const int* __restrict__ Na_sum, float rc2,
+                                   const float* __restrict__ box, const float* __restrict__ r, int* __restrict__ NN,
+                                   int* __restrict__ NL) {
+  const int c = blockIdx.x;
+  const int n_begin = Na_sum[c], n_end = n_begin + Na[c];
+  const float* h = box + 18 * (size_t)c;
+  float hh[18];
+#pragma unroll
+  for (int k = 0; k < 18; ++k) hh[k] = h[k];
+  for (int n1 = n_begin + threadIdx.x; n1 < n_end; n1 += blockDim.x) {
+    const float x1 = r[n1], y1 = r[n1 + N], z1 = r[n1 + 2 * (size_t)N];
+    int count = 0;
+    for (int n2 = n_begin; n2 < n_end; ++n2) {
+      if (n2 == n1) continue;
+      float x12 = __fsub_rn(r[n2], x1);
+      float y12 = __fsub_rn(r[n2 + N], y1);
+      float z12 = __fsub_rn(r[n2 + 2 * (size_t)N], z1);
+      float ix, iy, iz;
+      mic32<MODE>(hh, x12, y12, z12, ix, iy, iz);
+      const float d2 = dot3<MODE>(x12, x12, y12, y12, z12, z12);
+      if (d2 < rc2) NL[(size_t)count++ * N + n1] = n2;
+    }
+    NN[n1] = count;
+  }
+}
+
+constexpr double kRiAlpha = 0.2;                  // ri.cu:26
+constexpr double kRiPiFactor = 0.225675833419103;  // ri.cu:28, 2*alpha/sqrt(pi)
+
+// Per atom: FP64 bond vectors for the FP32-chosen image, FP32 unit vectors,
+// reverse bonds, half-list start and pair types.
+__global__ void bond_geometry(int N, const int* __restrict__ atom_cfg, const float* __restrict__ box,
+                              const float* __restrict__ r, const int* __restrict__ type, const int* __restrict__ off,
+                              const int* __restrict__ nbr, const float* __restrict__ img, int potential_type,
+                              int num_types, double4* __restrict__ g64, float4* __restrict__ g32,
+                              float4* __restrict__ gri, int* __restrict__ rev, int* __restrict__ half_off,
+                              uint8_t* __restrict__ ptype) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const float* h = box + 18 * (size_t)atom_cfg[i];
+  const double xi = r[i], yi = r[i + N], zi = r[i + 2 * (size_t)N];
+  int hstart = off[i + 1];
+  for (int b = off[i]; b < off[i + 1]; ++b) {
+    const int j = nbr[b];
+    const double ix = img[3 * (size_t)b], iy = img[3 * (size_t)b + 1], iz = img[3 * (size_t)b + 2];
+    double dx = (double)r[j] - xi, dy = (double)r[j + N] - yi, dz = (double)r[j + 2 * (size_t)N] - zi;
+    dx -= (double)h[0] * ix + (double)h[1] * iy + (double)h[2] * iz;
+    dy -= (double)h[3] * ix + (double)h[4] * iy + (double)h[5] * iz;
+    dz -= (double)h[6] * ix + (double)h[7] * iy + (double)h[8] * iz;
+    const double d = sqrt(dx * dx + dy * dy + dz * dz);
+    g64[b] = make_double4(dx, dy, dz, d);
+    g32[b] = make_float4((float)(dx / d), (float)(dy / d), (float)(dz / d), (float)d);
+    if (gri) {
+      const double dinv = 1.0 / d;
+      const double dinv3 = dinv * dinv * dinv;
+      const double e1 = erfc(kRiAlpha * d) * dinv;
+      const double e2 = e1 * dinv + kRiPiFactor * dinv * exp(-kRiAlpha * kRiAlpha * d * d);
+      gri[b] = make_float4((float)dinv, (float)(dinv3 * dinv3), (float)e1, (float)e2);
+    }
+    int rb = off[j];  // minimal_tersoff.cu:368: slot 0 when the reverse is absent
+    for (int k = off[j]; k < off[j + 1]; ++k)
+      if (nbr[k] == i) {
+        rb = k;
+        break;
+      }
+    rev[b] = rb;
+    if (j > i && hstart == off[i + 1]) hstart = b;
+    uint8_t t = 0;
+    if (potential_type == 0) t = (uint8_t)(type[i] + type[j]);
+    else if (num_types == 2) t = (uint8_t)(type[i] != type[j]);
+    ptype[b] = t;
+  }
+  half_off[i] = hstart;
+}
+
+// Three-body cosines cos(theta_jik) for every ordered pair of atom i's bonds.
+__global__ void triplet_cosines(int N, const int* __restrict__ off, const int* __restrict__ trip_off,
+                                const double4* __restrict__ g64, float* __restrict__ cosm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int b0 = off[i], Z = off[i + 1] - b0;
+  float* out = cosm + trip_off[i];
+  for (int j = 0; j < Z; ++j) {
+    const double4 a = g64[b0 + j];
+    for (int k = 0; k < Z; ++k) {
+      const double4 b = g64[b0 + k];
+      out[j * Z + k] = (float)((a.x * b.x + a.y * b.y + a.z * b.z) / (a.w * b.w));
+    }
+  }
+}
+
+int neighbor_reference_layout(int Nc, int N, int max_Na, const int* Na, const int* Na_sum, const float* r,
+                              const float* h, float cutoff, int* NN, int* NL, cudaStream_t st) {
+  (void)max_Na;
+  const float rc2 = cutoff * cutoff;  // neighbor.cu:73 (FP32 on the host)
+  neighbor_reference<kMicMode><<<Nc, 256, 0, st>>>(N, Na, Na_sum, rc2, h, r, NN, NL);
+  GPUGA_CUDA(cudaGetLastError());
+  return GPUGA_OK;
+}
+
+int build_geometry(Engine* e) {
+  DevSet& d = e->d;
+  const TrainingSet& ts = e->ts;
+  const int N = ts.N, Nc = ts.Nc;
+  cudaStream_t st = e->stream;
+  const float rc2 = e->spec.cutoff * e->spec.cutoff;
+
+  GPUGA_TRY(e->alloc(&d.NN, N));
+  GPUGA_TRY(e->alloc(&d.off, N + 1));
+  neighbor_scan<kMicMode, false><<<Nc, 256, 0, st>>>(N, d.Na, d.Na_sum, rc2, d.h, d.r, d.NN, nullptr, nullptr,
+                                                    nullptr);
+  GPUGA_CUDA(cudaGetLastError());
+  e->h_NN.assign(N, 0);
+  GPUGA_CUDA(cudaMemcpyAsync(e->h_NN.data(), d.NN, sizeof(int) * N, cudaMemcpyDeviceToHost, st));
+  GPUGA_CUDA(cudaStreamSynchronize(st));
+  e->h_off.assign(N + 1, 0);
+  long long total = 0;
+  int max_Z = 0;
+  for (int i = 0; i < N; ++i) {
+    e->h_off[i] = (int)total;
+    total += e->h_NN[i];
+    max_Z = std::max(max_Z, e->h_NN[i]);
+  }
+  if (total > (1LL << 31) - 1) {
+    set_error("neighbor list has %lld bonds, more than the engine indexes with int32.", total);
+    return GPUGA_ERR_UNSUPPORTED;
+  }
+  e->h_off[N] = (int)total;
+  const int B = (int)total;
+  d.B = B;
+  d.max_Z = max_Z;
+  GPUGA_CUDA(cudaMemcpyAsync(d.off, e->h_off.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice, st));
+
+  float* img = nullptr;
+  GPUGA_CUDA(cudaMalloc(&img, sizeof(float) * 3 * (size_t)std::max(B, 1)));
+  GPUGA_TRY(e->alloc(&d.nbr, std::max(B, 1)));
+  neighbor_scan<kMicMode, true><<<Nc, 256, 0, st>>>(N, d.Na, d.Na_sum, rc2, d.h, d.r, d.NN, d.off, d.nbr, img);
+  GPUGA_CUDA(cudaGetLastError());
+
+  // per-atom config index for the geometry kernel
+  std::vector<int> atom_cfg(N);
+  for (int c = 0; c < Nc; ++c)
+    for (int k = 0; k < ts.Na[c]; ++k) atom_cfg[ts.Na_sum[c] + k] = c;
+  int* d_atom_cfg = nullptr;
+  GPUGA_CUDA(cudaMalloc(&d_atom_cfg, sizeof(int) * N));
+  GPUGA_CUDA(cudaMemcpyAsync(d_atom_cfg, atom_cfg.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
+
+  GPUGA_TRY(e->alloc(&d.g64, std::max(B, 1)));
+  GPUGA_TRY(e->alloc(&d.g32, std::max(B, 1)));
+  GPUGA_TRY(e->alloc(&d.rev, std::max(B, 1)));
+  GPUGA_TRY(e->alloc(&d.half_off, N));
+  GPUGA_TRY(e->alloc(&d.ptype, std::max(B, 1)));
+  if (d.potential_type == 0) GPUGA_TRY(e->alloc(&d.gri, std::max(B, 1)));
+  bond_geometry<<<(N + 127) / 128, 128, 0, st>>>(N, d_atom_cfg, d.h, d.r, d.type, d.off, d.nbr, img,
+                                                 d.potential_type, d.num_types, d.g64, d.g32, d.gri, d.rev,
+                                                 d.half_off, d.ptype);
+  GPUGA_CUDA(cudaGetLastError());
+
+  if (d.potential_type == 1 || d.potential_type == 2) {
+    std::vector<int> trip(N + 1, 0);
+    long long t = 0;
+    for (int i = 0; i < N; ++i) {
+      trip[i] = (int)t;
+      t += (long long)e->h_NN[i] * e->h_NN[i];
+    }
+    if (t > (1LL << 31) - 1) {
+      set_error("too many three-body terms (%lld).", t);
+      return GPUGA_ERR_UNSUPPORTED;
+    }
+    trip[N] = (int)t;
+    GPUGA_TRY(e->alloc(&d.trip_off, N + 1));
+    GPUGA_TRY(e->alloc(&d.cosm, std::max<long long>(t, 1)));
+    GPUGA_CUDA(cudaMemcpyAsync(d.trip_off, trip.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice, st));
+    triplet_cosines<<<(N + 127) / 128, 128, 0, st>>>(N, d.off, d.trip_off, d.g64, d.cosm);
+    GPUGA_CUDA(cudaGetLastError());
+  }
+  GPUGA_CUDA(cudaStreamSynchronize(st));
+  cudaFree(img);
+  cudaFree(d_atom_cfg);
+
+  e->h_nbr.assign(std::max(B, 1), 0);
+  GPUGA_CUDA(cudaMemcpy(e->h_nbr.data(), d.nbr, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost));
+  e->h_zmax.assign(Nc, 0);
+  for (int c = 0; c < Nc; ++c)
+    for (int k = 0; k < ts.Na[c]; ++k) e->h_zmax[c] = std::max(e->h_zmax[c], e->h_NN[ts.Na_sum[c] + k]);
+  return GPUGA_OK;
+}
+
+}  // namespace gpuga

@@ -1,0 +1,218 @@
+/*
+ * gpuga.h -- C ABI of the B200 GPUGA fitness engine (libgpuga_b200.so).
+ *
+ * Plain C types only: pointers, sizes, status codes.  Every call returns an
+ * int status (GPUGA_OK == 0, negative on failure); gpuga_last_error() gives
+ * the message of the last failure on the calling thread.  Host buffers are
+ * caller-owned; device buffers are engine-owned unless a function says it
+ * takes device pointers.
+ *
+ * Each entry point names the reference interface it replaces
+ * (GPUGA, src/<file>:<line>).
+ */
+#ifndef GPUGA_B200_H
+#define GPUGA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define GPUGA_OK 0
+#define GPUGA_ERR_IO (-1)          /* file cannot be opened (error.cu:27-48 my_fopen) */
+#define GPUGA_ERR_PARSE (-2)       /* malformed or invalid input (fitness.cu:59-314, ga.cu:214-316) */
+#define GPUGA_ERR_UNSUPPORTED (-3) /* potential_type / size outside what the engine supports */
+#define GPUGA_ERR_OOM (-4)         /* device or host allocation failed */
+#define GPUGA_ERR_CUDA (-5)        /* a CUDA call failed (error.cuh:35-51 CHECK) */
+#define GPUGA_ERR_TIMEOUT (-6)     /* a bounded device wait gave up */
+#define GPUGA_ERR_NAN (-7)         /* non-finite fitness where the caller asked for a check */
+#define GPUGA_ERR_ARG (-8)         /* invalid argument */
+#define GPUGA_ERR_BUDGET (-9)      /* serving: job larger than the HBM budget */
+#define GPUGA_ERR_CANCELLED (-10)  /* serving: job was cancelled */
+#define GPUGA_ERR_NOT_READY (-11)  /* serving: job still running */
+
+/* Evaluation paths. */
+#define GPUGA_PATH_BATCHED 0 /* all individuals x all configs per generation, FP32 math + FP64 sums */
+#define GPUGA_PATH_PLAIN64 1 /* one individual per launch, FP64 throughout */
+#define GPUGA_PATH_PLAIN32 2 /* one individual per launch, FP32 throughout (reference-like) */
+
+typedef struct gpuga_engine gpuga_engine;
+typedef struct gpuga_ga gpuga_ga;
+typedef struct gpuga_server gpuga_server;
+typedef struct gpuga_potential gpuga_potential;
+
+typedef struct gpuga_options {
+  int device;          /* CUDA device ordinal */
+  int path;            /* GPUGA_PATH_* used by gpuga_fitness */
+  int use_graph;       /* capture each generation in a CUDA graph (batched path) */
+  int nn2b_consistent; /* 1: taper the NN2B force consistently (fixes nn2b.cu:147-148) */
+  float nn2b_r1;       /* NN2B taper start, reference default 7 (nn2b.cuh:36) */
+  float nn2b_r2;       /* NN2B taper end, reference default 8 (nn2b.cuh:37) */
+  int verbose;         /* print the reference's start-up banners */
+} gpuga_options;
+
+/* Fills *opt with the reference's semantics (batched path, graphs on, NN2B taper 7..8 A, force quirk kept). */
+void gpuga_default_options(gpuga_options* opt);
+
+const char* gpuga_last_error(void);
+const char* gpuga_version(void);
+
+/* --------------------------------------------------------------- engine set-up */
+/* Replaces Fitness::Fitness(char*) (fitness.cu:30-38): reads <dir>/potential.in and
+ * <dir>/train.in, builds the neighbor list on the GPU (bit-exact with neighbor.cu:30-66)
+ * and uploads the training set. */
+int gpuga_engine_create(const char* dir, const gpuga_options* opt, gpuga_engine** out);
+
+/* Same, from in-memory arrays laid out as the reference stores them after parsing
+ * (fitness.cu:59-161): r is SoA float[3N]; box9 is float[9*Nc] as written in train.in
+ * (row k of the file matrix = 3 consecutive floats, transposed into h like fitness.cu:115-123);
+ * pe_ref float[Nc]; virial_ref float[6*Nc] ([c + Nc*k]); force_ref float[3N] SoA.
+ * pmin/pmax float[num_vars]; weights = {force, energy, stress}. */
+int gpuga_engine_create_from_arrays(int potential_type, int num_neurons, float cutoff, const float* weights,
+                                    const float* pmin, const float* pmax, int Nc, int Nc_force, const int* Na,
+                                    const int* type, const float* r, const float* box9, const float* pe_ref,
+                                    const float* virial_ref, const float* force_ref, const gpuga_options* opt,
+                                    gpuga_engine** out);
+
+int gpuga_engine_destroy(gpuga_engine* e);
+
+/* Parses <dir>/potential.in, train.in and (if present) ga.in with the reference's rules
+ * (fitness.cu:59-314, ga.cu:214-316) without touching the GPU.  sizes (may be NULL):
+ * potential_type, num_vars, num_neurons, Nc, Nc_force, N, N_force, max_Na,
+ * population_size, parent_number, maximum_generation. */
+int gpuga_parse_inputs(const char* dir, int* sizes11);
+
+/* sizes: potential_type, num_vars, num_neurons, Nc, Nc_force, N, N_force, max_Na, num_bonds, max_neighbors */
+int gpuga_engine_info(const gpuga_engine* e, int* sizes10);
+/* Parameter bounds (fitness.cuh:37-38) */
+int gpuga_engine_bounds(const gpuga_engine* e, float* pmin, float* pmax);
+/* FP64 normalisers of the relative RMSEs (fitness.cu:86-160): {force, energy, virial} */
+int gpuga_engine_norms(const gpuga_engine* e, double* norms3);
+
+/* Neighbor list as the reference stores it (neighbor.cu:61): NN int[N], NL int[max_Na*N], NL[k*N+i]. */
+int gpuga_engine_neighbors(const gpuga_engine* e, int* NN, int* NL);
+/* Same list in CSR form: NN int[N], nbr int[num_bonds] (ascending global indices per atom). */
+int gpuga_engine_neighbors_csr(const gpuga_engine* e, int* NN, int* nbr);
+
+/* ------------------------------------------------------------- fitness (hot path) */
+/* Replaces Fitness::compute(int, float*, float*) (fitness.cu:316-333).
+ * pop01: host float[P*num_vars] in [0,1]; fitness_out: host double[P].
+ * Synchronous on return.  Uses opt.path. */
+int gpuga_fitness(gpuga_engine* e, int P, const float* pop01, double* fitness_out);
+
+/* Same with an explicit path and the three relative RMSEs per individual
+ * (components_out double[3P] as {energy, virial, force}; may be NULL). */
+int gpuga_fitness_ex(gpuga_engine* e, int path, int P, const float* pop01, double* fitness_out,
+                     double* components_out);
+
+/* Batched path on device-resident buffers (no host copies): d_pop01 device float[P*num_vars],
+ * d_fitness device double[P].  Enqueued on `stream` (a cudaStream_t, NULL = legacy default);
+ * returns without synchronising. */
+int gpuga_fitness_device(gpuga_engine* e, int P, const float* d_pop01, double* d_fitness, void* stream);
+
+/* Per-(individual, config) results of the last batched evaluation:
+ * energy double[P*Nc], virial double[P*Nc*6] ([p][c][k], k = xx,yy,zz,xy,yz,zx; E/V configs only),
+ * force_sq double[P*Nc] (sum |F-F_ref|^2 of the config's atoms; force configs only).  Any may be NULL. */
+int gpuga_last_config_results(gpuga_engine* e, int P, double* energy, double* virial, double* force_sq);
+
+/* Per-atom forces of the force configurations from the batched path for P individuals:
+ * forces_out host float[P*3*N_force] ([p][xyz][i]).  Evaluates the population. */
+int gpuga_batched_forces(gpuga_engine* e, int P, const float* pop01, float* forces_out);
+
+/* Launch plan of the batched path for population size P (built on first use).
+ * *n_launches = batched force launches per generation (decode and fitness-fold launches come on top);
+ * per_launch (may be NULL) receives up to `cap` rows of 8 doubles:
+ * {kind (0 Tersoff, 1 RI, 2 NN2B), register class, force items?, CTAs, (individual, atom) units,
+ *  algorithmic FP32 flops, transcendental calls, mean device ms per generation while timing is on}. */
+int gpuga_plan_info(gpuga_engine* e, int P, int* n_launches, double* per_launch, int cap);
+/* Records CUDA events around every batched launch of population size P on the launch's own
+ * stream (eager launches only: gpuga_fitness_device, or gpuga_fitness with use_graph = 0);
+ * enabling or disabling resets the accumulated times. */
+int gpuga_kernel_timing(gpuga_engine* e, int P, int enable);
+/* Measured FP32 CUDA-core FMA throughput of `device` (TFLOP/s), for roofline fractions. */
+int gpuga_calibrate_fp32(int device, double* tflops);
+
+/* Replaces Potential::update_potential + Potential::find_force (potential.cuh:22-41) for one
+ * decoded parameter vector (potential.in order).  FP64 path: F double[3N], W double[6N], pe double[N]
+ * (SoA, virial order xx,yy,zz,xy,yz,zx). */
+int gpuga_find_force64(gpuga_engine* e, const double* params, double* F, double* W, double* pe);
+/* FP32 path with the reference's float outputs. */
+int gpuga_find_force32(gpuga_engine* e, const float* params, float* F, float* W, float* pe);
+
+/* Replaces Fitness::predict(char*, float*) (fitness.cu:335-390): decodes elite01 (float[num_vars])
+ * in FP32, evaluates it on the FP64 path and writes <dir>/force.out, energy.out, virial.out in
+ * the reference's "%g" format. */
+int gpuga_predict(gpuga_engine* e, const char* dir, const float* elite01);
+
+/* Decode x in [0,1] to parameters exactly like fitness.cu:320-324 (FP32, no contraction). */
+int gpuga_decode(const gpuga_engine* e, const float* x01, float* params);
+
+/* -------------------------------------------------------------------- GA (ga.cu) */
+/* Replaces GA::GA + GA::compute (ga.cu:27-92) one generation at a time.
+ * Reads <dir>/ga.in (ga.cu:214-316).  seed: std::mt19937 seed (12345678 = the reference's -DDEBUG). */
+int gpuga_ga_create(gpuga_engine* e, const char* dir, unsigned seed, gpuga_ga** out);
+/* Same with explicit ga.in values. */
+int gpuga_ga_create_params(gpuga_engine* e, int population_size, int parent_number, float mutation_rate,
+                           int maximum_generation, unsigned seed, gpuga_ga** out);
+/* Host-only GA (no engine) whose fitness comes from a caller callback: fitness_cb(P, pop01, fitness_out, user). */
+typedef void (*gpuga_fitness_cb)(int P, const float* pop01, float* fitness_out, void* user);
+int gpuga_ga_create_host(int num_vars, const float* pmin, const float* pmax, int population_size,
+                         int parent_number, float mutation_rate, int maximum_generation, unsigned seed,
+                         gpuga_fitness_cb cb, void* user, gpuga_ga** out);
+/* One generation: evaluate, sort, output line, crossover, mutation (ga.cu:82-88).
+ * line_out (may be NULL) receives the ga.out line for this generation. */
+int gpuga_ga_step(gpuga_ga* g, char* line_out, int line_len);
+/* Runs all remaining generations writing <dir>/ga.out, then predict() (ga.cu:73-92). */
+int gpuga_ga_run(gpuga_ga* g, const char* dir);
+/* population_out float[P*num_vars] (sorted after the last step), fitness_out float[P] */
+int gpuga_ga_state(const gpuga_ga* g, int* generation, float* population_out, float* fitness_out);
+int gpuga_ga_destroy(gpuga_ga* g);
+
+/* ----------------------------------------------------- reference Potential drop-in */
+/* A stand-alone potential that evaluates on caller-provided DEVICE arrays in the reference's
+ * layouts, for a maintainer who keeps the reference's Fitness/Neighbor and swaps the force kernel.
+ * Replaces Minimal_Tersoff/RI/NN2B (minimal_tersoff.cu, ri.cu, nn2b.cu). */
+int gpuga_potential_create(int potential_type, int num_neurons, gpuga_potential** out);
+/* Potential::initialize(N, max_Na) (potential.cuh:25) */
+int gpuga_potential_initialize(gpuga_potential* p, int N, int max_Na);
+/* Potential::update_potential(const std::vector<float>&) (potential.cuh:26) */
+int gpuga_potential_update(gpuga_potential* p, const float* params, int num_params);
+/* Potential::find_force (potential.cuh:28-40); every pointer is a device pointer in the reference
+ * layout (NL[k*N+i], r SoA, h 18 floats per config, f SoA 3N, virial 6N, pe N). */
+int gpuga_potential_find_force(gpuga_potential* p, int Nc, int N, const int* Na, const int* Na_sum, int max_Na,
+                               const int* type, const float* h, const int* NN, const int* NL, const float* r,
+                               float* f, float* virial, float* pe, void* stream);
+int gpuga_potential_destroy(gpuga_potential* p);
+/* Neighbor::compute (neighbor.cu:68-83) on device arrays: NN int[N], NL int[max_Na*N]. */
+int gpuga_neighbor_compute(int Nc, int N, int max_Na, const int* Na, const int* Na_sum, const float* r,
+                           const float* h, float cutoff, int* NN, int* NL, void* stream);
+
+/* ------------------------------------------------------------------ serving */
+/* A device-resident server that runs many fitting jobs concurrently, admitting jobs while the
+ * sum of their device footprints stays within hbm_budget_bytes and batching the generations of
+ * all running jobs into shared launches.  No reference counterpart (the reference fits one
+ * potential per process, main.cu:25-55). */
+int gpuga_server_create(int device, double hbm_budget_bytes, int max_jobs, gpuga_server** out);
+/* Submits a fitting job for <dir> (potential.in, train.in, ga.in).  generations <= 0 uses ga.in.
+ * Returns the job id in *job_id. */
+int gpuga_server_submit(gpuga_server* s, const char* dir, unsigned seed, int generations, int* job_id);
+/* Submits a job from an existing engine's training set (shared, not copied). */
+int gpuga_server_submit_engine(gpuga_server* s, gpuga_engine* e, int population_size, int parent_number,
+                               float mutation_rate, int generations, unsigned seed, int* job_id);
+/* Status of a job: GPUGA_OK when finished, GPUGA_ERR_NOT_READY while queued/running, or its error.
+ * progress_out (may be NULL): {generations done, generations total, state(0 queued,1 running,2 done,3 failed,4 cancelled)} */
+int gpuga_server_poll(gpuga_server* s, int job_id, int* progress_out);
+/* Best fitness history and final elite of a finished job: best_out float[generations], elite01_out float[num_vars] */
+int gpuga_server_result(gpuga_server* s, int job_id, float* best_out, float* elite01_out);
+int gpuga_server_cancel(gpuga_server* s, int job_id);
+/* Runs the scheduler until every submitted job is finished (or timeout_s elapses, -> GPUGA_ERR_TIMEOUT). */
+int gpuga_server_drain(gpuga_server* s, double timeout_s);
+/* stats: {generation batches run, jobs finished, p50 gen latency ms, p99 gen latency ms,
+ *         aggregate evals/s, device bytes in use, peak jobs resident, total evals} */
+int gpuga_server_stats(gpuga_server* s, double* stats8);
+int gpuga_server_destroy(gpuga_server* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUGA_B200_H */
