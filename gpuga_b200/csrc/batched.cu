@@ -21,6 +21,7 @@
 // is parameter-independent and precomputed once (geometry.cu).
 #include <algorithm>
 #include <cmath>
+#include <tuple>
 
 #include "engine.hpp"
 
@@ -45,14 +46,20 @@ __device__ __forceinline__ float decode1(float mn, float mx, float x) {
   return __fadd_rn(mn, __fmul_rn(__fsub_rn(mx, mn), x));  // fitness.cu:320-324, no contraction
 }
 
-// One thread per individual: FP32 decode exactly like the reference, derived
-// constants in FP64 rounded once to FP32.
-__global__ void decode_population(int P, int nv, int potential_type, int num_types, const float* __restrict__ pop,
-                                  const float* __restrict__ pmin, const float* __restrict__ pmax, int Pstride,
-                                  float* __restrict__ consts, float* __restrict__ weights) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P) return;
-  const float* x = pop + (size_t)p * nv;
+// One thread per individual of every job of the set: FP32 decode exactly like
+// the reference, derived constants in FP64 rounded once to FP32.
+__global__ void decode_jobs(const JobView* __restrict__ jobs, const int2* __restrict__ indmap, int total) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  const int2 jp = indmap[t];
+  const JobView& J = jobs[jp.x];
+  const int p = jp.y, nv = J.num_vars, Pstride = J.Pstride, potential_type = J.potential_type;
+  const int num_types = J.num_types;
+  const float* __restrict__ pmin = J.pmin;
+  const float* __restrict__ pmax = J.pmax;
+  float* __restrict__ consts = J.consts;
+  float* __restrict__ weights = J.weights;
+  const float* x = J.pop + (size_t)p * nv;
   auto par = [&](int m) { return (double)decode1(pmin[m], pmax[m], x[m]); };
   auto put = [&](int k, double v) { consts[(size_t)k * Pstride + p] = (float)v; };
   if (potential_type == 1 || potential_type == 2) {
@@ -148,22 +155,6 @@ __device__ __forceinline__ void cutoff_fn(float r1, float r2, float pf, float d,
     fcp = 0.0f;
   }
 }
-
-struct DevView {
-  int Nc, N, N_force;
-  const int* Na;
-  const int* Na_sum;
-  const int* NN;
-  const int* off;
-  const int* half_off;
-  const int* trip_off;
-  const int* rev;
-  const uint8_t* ptype;
-  const float4* g32;
-  const float4* gri;
-  const float* cosm;
-  const float* force_ref;
-};
 
 // Block-wide fixed-order reduction of the per-lane accumulators into res[p][c][k].
 __device__ __forceinline__ void reduce_item(const WorkItem& it, int P, int Nc, double (&acc)[kResK],
@@ -307,16 +298,20 @@ __device__ __forceinline__ float tersoff_atom(const DevView& S, const TersoffC& 
 }
 
 template <int ZC, bool FORCE>
-__global__ void __launch_bounds__(kBlock) tersoff_batched(DevView S, const WorkItem* __restrict__ items,
-                                                          const float* __restrict__ consts, int Pstride, int P,
-                                                          double* __restrict__ res, float* __restrict__ fdump) {
+__global__ void __launch_bounds__(kBlock) tersoff_batched(const JobView* __restrict__ jobs,
+                                                          const WorkItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem[];
   const WorkItem it = items[blockIdx.x];
+  const JobView& J = jobs[it.job];
+  const DevView S = J.v;
+  const int P = J.P;
+  double* __restrict__ res = J.res;
+  float* __restrict__ fdump = J.fdump;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int G = it.G, A = 32 / G;
   const int g = lane & (G - 1), aslot = lane / G;
   const int p = it.p0 + g;
-  const Consts kc{consts, Pstride, p < P ? p : it.p0};
+  const Consts kc{J.consts, J.Pstride, p < P ? p : it.p0};
   TersoffC C;
   load_tersoff(kc, C);
   const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
@@ -424,22 +419,22 @@ __device__ __forceinline__ void nn_pair(const float* __restrict__ wl, int n, flo
   p2 -= wl[(n * (n + 4)) * 32];
 }
 
-struct NNTaper {
-  float r1, r2, pf;
-  int consistent;
-};
-
 template <int KIND, int NMAX, bool FORCE>
-__global__ void __launch_bounds__(kBlock) pair_batched(DevView S, const WorkItem* __restrict__ items,
-                                                       const float* __restrict__ consts,
-                                                       const float* __restrict__ weights, int Pstride, int P,
-                                                       int nn, int nv, NNTaper tp, double* __restrict__ res) {
+__global__ void __launch_bounds__(kBlock) pair_batched(const JobView* __restrict__ jobs,
+                                                       const WorkItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem[];
   const WorkItem it = items[blockIdx.x];
+  const JobView& J = jobs[it.job];
+  const DevView S = J.v;
+  const int P = J.P, Pstride = J.Pstride, nn = J.num_neurons, nv = J.num_vars;
+  const NNTaper tp = J.tp;
+  const float* __restrict__ weights = J.weights;
+  double* __restrict__ res = J.res;
+  float* __restrict__ fdump = J.fdump;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int p = it.p0 + lane;
   const int pl = p < P ? p : it.p0;
-  const Consts kc{consts, Pstride, pl};
+  const Consts kc{J.consts, Pstride, pl};
   float* wsm = reinterpret_cast<float*>(smem + (size_t)kWarps * 32 * kResK * sizeof(double));
   if (KIND == 2) {
     for (int t = threadIdx.x; t < nv * 32; t += blockDim.x) {
@@ -501,20 +496,34 @@ __global__ void __launch_bounds__(kBlock) pair_batched(DevView S, const WorkItem
       const double dy = Fy - (double)S.force_ref[i + N];
       const double dz = Fz - (double)S.force_ref[i + 2 * (size_t)N];
       acc[7] += dx * dx + dy * dy + dz * dz;
+      if (fdump && p < P) {
+        const int Nf = S.N_force;
+        fdump[((size_t)p * 3 + 0) * Nf + i] = (float)Fx;
+        fdump[((size_t)p * 3 + 1) * Nf + i] = (float)Fy;
+        fdump[((size_t)p * 3 + 2) * Nf + i] = (float)Fz;
+      }
     }
   }
   reduce_item(it, P, S.Nc, acc, smem, res);
 }
 
 // --------------------------------------------------------------------------- fitness
-// fitness.cu:329-331, 437-555 in FP64: one warp per individual, fixed-order sums.
-__global__ void fitness_reduce(int P, int Nc, int Nc_force, const double* __restrict__ res,
-                               const double* __restrict__ E_ref, const double* __restrict__ W_ref, double nF,
-                               double nE, double nW, float wF, float wE, float wW, double* __restrict__ fitness,
-                               double* __restrict__ comps) {
-  const int p = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+// fitness.cu:329-331, 437-555 in FP64: one warp per individual of every job,
+// fixed-order sums.
+__global__ void fitness_jobs(const JobView* __restrict__ jobs, const int2* __restrict__ indmap, int total) {
+  const int t = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (p >= P) return;
+  if (t >= total) return;
+  const int2 jp = indmap[t];
+  const JobView& J = jobs[jp.x];
+  const int p = jp.y, Nc = J.v.Nc, Nc_force = J.Nc_force;
+  const double* __restrict__ res = J.res;
+  const double* __restrict__ E_ref = J.E_ref;
+  const double* __restrict__ W_ref = J.W_ref;
+  const double nF = J.nF, nE = J.nE, nW = J.nW;
+  const float wF = J.wF, wE = J.wE, wW = J.wW;
+  double* __restrict__ fitness = J.fitness;
+  double* __restrict__ comps = J.comps;
   double eE = 0, eW = 0, eF = 0;
   for (int c = lane; c < Nc; c += 32) {
     const double* r = res + ((size_t)p * Nc + c) * kResK;
@@ -577,29 +586,87 @@ DevView make_view(const DevSet& d) {
   return v;
 }
 
-static int launch_one(Engine* e, Plan* plan, const Launch& L, cudaStream_t st, bool configure_only);
+JobView make_job_view(const Engine* e, const Plan* plan) {
+  const DevSet& d = e->d;
+  JobView j{};
+  j.v = make_view(d);
+  j.potential_type = d.potential_type;
+  j.num_types = d.num_types;
+  j.num_neurons = d.num_neurons;
+  j.num_vars = d.num_vars;
+  j.P = plan->P;
+  j.Pstride = plan->Pstride;
+  j.Nc_force = d.Nc_force;
+  j.tp = NNTaper{e->spec.nn_r1, e->spec.nn_r2, (float)(M_PI / ((double)e->spec.nn_r2 - e->spec.nn_r1)),
+                 e->spec.nn_consistent};
+  j.pop = plan->d_pop;
+  j.pmin = e->d_pmin;
+  j.pmax = e->d_pmax;
+  j.consts = plan->d_consts;
+  j.weights = plan->d_weights;
+  j.res = plan->d_res;
+  j.fdump = plan->dump ? plan->d_fdump : nullptr;
+  j.E_ref = d.E_ref;
+  j.W_ref = d.W_ref;
+  j.nF = d.norm_force;
+  j.nE = d.norm_energy;
+  j.nW = d.norm_virial;
+  j.wF = d.w_force;
+  j.wE = d.w_energy;
+  j.wW = d.w_stress;
+  j.fitness = plan->d_fitness;
+  j.comps = plan->d_comps;
+  return j;
+}
 
-int plan_build(Engine* e, int P, Plan** out) {
+LaunchSet::~LaunchSet() {
+  if (d_jobs) cudaFree(d_jobs);
+  if (h_jobs) cudaFreeHost(h_jobs);
+  if (d_items) cudaFree(d_items);
+  if (d_indmap) cudaFree(d_indmap);
+  if (side) cudaStreamDestroy(side);
+  if (fork) cudaEventDestroy(fork);
+  if (join) cudaEventDestroy(join);
+  for (auto ev : tev)
+    if (ev) cudaEventDestroy(ev);
+}
+
+Plan::~Plan() {
+  if (graph) cudaGraphExecDestroy(graph);
+  if (h_pop) cudaFreeHost(h_pop);
+  if (h_fit) cudaFreeHost(h_fit);
+}
+
+namespace {
+
+struct ItemSpec {
+  WorkItem w;
+  double cost, units, flops, sfu;
+};
+struct LaunchKey {
+  int kind, zclass, nmax, force;
+  bool operator<(const LaunchKey& o) const {
+    return std::tie(kind, zclass, nmax, force) < std::tie(o.kind, o.zclass, o.nmax, o.force);
+  }
+};
+
+// Work items of one job, grouped by kernel.
+//   Algorithmic work per (individual, atom), counted on the batched formulation
+//   (FMA = 2 flops; exp/pow/erfc/tanh/sin-cos calls counted as SFU work):
+//     Tersoff: 60 flops + 4 transcendentals per bond, 21 flops per ordered triplet
+//     RI:      25 flops + 2 transcendentals per pair (Morse included on average)
+//     NN2B:    4n^2 + 13n + 10 flops + 2n tanh per pair
+int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<ItemSpec>>& groups,
+              std::map<LaunchKey, size_t>& smem_need) {
   const DevSet& d = e->d;
   const TrainingSet& ts = e->ts;
-  std::unique_ptr<Plan> plan(new Plan);
-  plan->P = P;
-  plan->Pstride = (P + 31) & ~31;
   const bool tersoff = d.potential_type == 1 || d.potential_type == 2;
   const int kind = tersoff ? 0 : (d.potential_type == 0 ? 1 : 2);
-  if (kind == 2 && nmax_of(d.num_neurons) == 0) {
+  const int nmax = kind == 2 ? nmax_of(d.num_neurons) : 0;
+  if (kind == 2 && nmax == 0) {
     set_error("batched NN2B supports up to 32 neurons per layer (got %d).", d.num_neurons);
     return GPUGA_ERR_UNSUPPORTED;
   }
-  struct Tmp {
-    WorkItem w;
-    double cost, units, flops, sfu;
-  };
-  // Algorithmic work per (individual, atom), counted on the batched formulation
-  // (FMA = 2 flops; exp/pow/erfc/tanh/sin-cos calls counted as SFU work):
-  //   Tersoff: 60 flops + 4 transcendentals per bond, 21 flops per ordered triplet
-  //   RI:      20 flops + 1 exp per pair (+10 flops + 2 exp for cation-anion Morse)
-  //   NN2B:    4n^2 + 13n + 10 flops + 2n tanh per pair
   std::vector<double> atom_flops(ts.N), atom_sfu(ts.N), atom_flops_half(ts.N), atom_sfu_half(ts.N);
   for (int i = 0; i < ts.N; ++i) {
     const double Z = e->h_NN[i];
@@ -618,15 +685,12 @@ int plan_build(Engine* e, int P, Plan** out) {
       atom_sfu_half[i] = spp * half;
     }
   }
-  std::map<std::pair<int, int>, std::vector<Tmp>> groups;  // (zclass, force) -> items
-  std::map<std::pair<int, int>, size_t> smem_need;
   for (int c = 0; c < ts.Nc; ++c) {
     const bool force = c < ts.Nc_force;
     const int Na = ts.Na[c];
     const long long Bc = (long long)e->h_off[ts.Na_sum[c] + Na] - e->h_off[ts.Na_sum[c]];
     int zc = 0, G = 32;
     size_t smem = kRedBytes;
-    double per_atom;
     if (kind == 0) {
       zc = zclass_of(e->h_zmax[c]);
       if (zc == 0) {
@@ -643,12 +707,10 @@ int plan_build(Engine* e, int P, Plan** out) {
         }
         smem = std::max(smem, per_ind * G);
       }
-      per_atom = (double)zc * zc + 8.0 * zc;
-    } else {
-      if (kind == 2) smem += (size_t)d.num_vars * 32 * sizeof(float);
-      per_atom = (double)Bc / Na * (force ? 1.0 : 0.5) * (kind == 2 ? 4.0 * d.num_neurons * d.num_neurons : 40.0);
+    } else if (kind == 2) {
+      smem += (size_t)d.num_vars * 32 * sizeof(float);
     }
-    auto key = std::make_pair(zc, force ? 1 : 0);
+    const LaunchKey key{kind, zc, nmax, force ? 1 : 0};
     smem_need[key] = std::max(smem_need[key], smem);
     double cf = 0, cs = 0;
     const bool half = kind != 0 && !force;
@@ -659,78 +721,38 @@ int plan_build(Engine* e, int P, Plan** out) {
     }
     for (int p0 = 0; p0 < P; p0 += G) {
       const int cnt = std::min(G, P - p0);
-      groups[key].push_back({WorkItem{c, p0, G, force ? 1 : 0}, per_atom * Na * cnt, (double)Na * cnt, cf * cnt,
-                             cs * cnt});
+      groups[key].push_back({WorkItem{c, p0, G, job}, cf * cnt, (double)Na * cnt, cf * cnt, cs * cnt});
     }
   }
-  size_t total = 0;
-  for (auto& kv : groups) total += kv.second.size();
-  GPUGA_TRY(e->alloc(&plan->d_items, std::max<size_t>(total, 1)));
-  std::vector<WorkItem> all;
-  all.reserve(total);
-  for (auto& kv : groups) {
-    auto& v = kv.second;
-    std::stable_sort(v.begin(), v.end(), [](const Tmp& a, const Tmp& b) { return a.cost > b.cost; });
-    Launch L;
-    L.kind = kind;
-    L.zclass = kv.first.first;
-    L.force = kv.first.second != 0;
-    L.smem = smem_need[kv.first];
-    L.count = (int)v.size();
-    L.d_items = plan->d_items + all.size();
-    for (auto& t : v) {
-      all.push_back(t.w);
-      L.units += t.units;
-      L.flops += t.flops;
-      L.sfu += t.sfu;
-    }
-    plan->launches.push_back(L);
-  }
-  // largest launches first so the side stream gets the long ones early
-  std::stable_sort(plan->launches.begin(), plan->launches.end(),
-                   [](const Launch& a, const Launch& b) { return a.count > b.count; });
-  GPUGA_CUDA(cudaMemcpy(plan->d_items, all.data(), sizeof(WorkItem) * all.size(), cudaMemcpyHostToDevice));
-  const int K = consts_per_individual(d);
-  GPUGA_TRY(e->alloc(&plan->d_consts, (size_t)K * plan->Pstride));
-  if (kind == 2) GPUGA_TRY(e->alloc(&plan->d_weights, (size_t)d.num_vars * plan->Pstride));
-  GPUGA_TRY(e->alloc(&plan->d_res, (size_t)P * d.Nc * kResK));
-  GPUGA_TRY(e->alloc(&plan->d_fitness, (size_t)P));
-  GPUGA_TRY(e->alloc(&plan->d_comps, (size_t)3 * P));
-  GPUGA_TRY(e->alloc(&plan->d_pop, (size_t)P * d.num_vars));
-  GPUGA_CUDA(cudaMallocHost(&plan->h_pop, sizeof(float) * (size_t)P * d.num_vars));
-  GPUGA_CUDA(cudaMallocHost(&plan->h_fit, sizeof(double) * 4 * (size_t)P));
-  GPUGA_CUDA(cudaStreamCreateWithFlags(&plan->side, cudaStreamNonBlocking));
-  GPUGA_CUDA(cudaEventCreateWithFlags(&plan->fork, cudaEventDisableTiming));
-  GPUGA_CUDA(cudaEventCreateWithFlags(&plan->join, cudaEventDisableTiming));
-  plan->tev.assign(2 * plan->launches.size(), nullptr);
-  for (auto& ev : plan->tev) GPUGA_CUDA(cudaEventCreate(&ev));
-  plan->t_ms.assign(plan->launches.size(), 0.0);
-  for (const Launch& L : plan->launches) GPUGA_TRY(launch_one(e, plan.get(), L, nullptr, true));
-  *out = plan.release();
   return GPUGA_OK;
 }
 
 template <class K>
-static int set_smem(K kernel, size_t smem) {
-  GPUGA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(smem, kSmemMax)));
+int set_smem(K kernel) {
+  GPUGA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
   return GPUGA_OK;
 }
 
-// configure_only: set the dynamic shared-memory limit of the launch's kernel
-// (done once when the plan is built, never inside a stream capture).
-static int launch_one(Engine* e, Plan* plan, const Launch& L, cudaStream_t st, bool configure_only) {
-  const DevSet& d = e->d;
-  const DevView v = make_view(d);
-  const int P = plan->P;
+// configure_only: raise the dynamic shared-memory limit of the launch's kernel
+// (done when a launch set is built, never inside a stream capture).
+int launch_one(const LaunchSet* ls, const Launch& L, cudaStream_t st, bool configure_only) {
   const dim3 grid(L.count), block(kBlock);
-#define GPUGA_TERSOFF(ZC, F)                                                                           \
-  do {                                                                                                 \
-    if (configure_only) {                                                                              \
-      GPUGA_TRY(set_smem(tersoff_batched<ZC, F>, L.smem));                                             \
-      break;                                                                                           \
-    }                                                                                                  \
-    tersoff_batched<ZC, F><<<grid, block, L.smem, st>>>(v, L.d_items, plan->d_consts, plan->Pstride, P, \
-                                                        plan->d_res, plan->dump ? plan->d_fdump : nullptr);                  \
+  const WorkItem* items = ls->d_items + L.first;
+#define GPUGA_TERSOFF(ZC, F)                                                          \
+  do {                                                                                \
+    if (configure_only) {                                                             \
+      GPUGA_TRY(set_smem(tersoff_batched<ZC, F>));                                    \
+      break;                                                                          \
+    }                                                                                 \
+    tersoff_batched<ZC, F><<<grid, block, L.smem, st>>>(ls->d_jobs, items);           \
+  } while (0)
+#define GPUGA_PAIR(KD, NM, F)                                                         \
+  do {                                                                                \
+    if (configure_only) {                                                             \
+      GPUGA_TRY(set_smem(pair_batched<KD, NM, F>));                                   \
+      break;                                                                          \
+    }                                                                                 \
+    pair_batched<KD, NM, F><<<grid, block, L.smem, st>>>(ls->d_jobs, items);          \
   } while (0)
   if (L.kind == 0) {
     if (L.zclass == 4) {
@@ -740,31 +762,14 @@ static int launch_one(Engine* e, Plan* plan, const Launch& L, cudaStream_t st, b
     } else {
       if (L.force) GPUGA_TERSOFF(16, true); else GPUGA_TERSOFF(16, false);
     }
+  } else if (L.kind == 1) {
+    if (L.force) GPUGA_PAIR(1, 8, true); else GPUGA_PAIR(1, 8, false);
+  } else if (L.nmax == 8) {
+    if (L.force) GPUGA_PAIR(2, 8, true); else GPUGA_PAIR(2, 8, false);
+  } else if (L.nmax == 16) {
+    if (L.force) GPUGA_PAIR(2, 16, true); else GPUGA_PAIR(2, 16, false);
   } else {
-    NNTaper tp{e->spec.nn_r1, e->spec.nn_r2, (float)(M_PI / ((double)e->spec.nn_r2 - e->spec.nn_r1)),
-               e->spec.nn_consistent};
-#define GPUGA_PAIR(KD, NM, F)                                                                           \
-  do {                                                                                                  \
-    if (configure_only) {                                                                               \
-      GPUGA_TRY(set_smem(pair_batched<KD, NM, F>, L.smem));                                             \
-      break;                                                                                            \
-    }                                                                                                   \
-    pair_batched<KD, NM, F><<<grid, block, L.smem, st>>>(v, L.d_items, plan->d_consts, plan->d_weights, \
-                                                         plan->Pstride, P, d.num_neurons, d.num_vars, tp,   \
-                                                         plan->d_res);                                  \
-  } while (0)
-    if (L.kind == 1) {
-      if (L.force) GPUGA_PAIR(1, 8, true); else GPUGA_PAIR(1, 8, false);
-    } else {
-      const int nm = nmax_of(d.num_neurons);
-      if (nm == 8) {
-        if (L.force) GPUGA_PAIR(2, 8, true); else GPUGA_PAIR(2, 8, false);
-      } else if (nm == 16) {
-        if (L.force) GPUGA_PAIR(2, 16, true); else GPUGA_PAIR(2, 16, false);
-      } else {
-        if (L.force) GPUGA_PAIR(2, 32, true); else GPUGA_PAIR(2, 32, false);
-      }
-    }
+    if (L.force) GPUGA_PAIR(2, 32, true); else GPUGA_PAIR(2, 32, false);
   }
 #undef GPUGA_TERSOFF
 #undef GPUGA_PAIR
@@ -772,53 +777,137 @@ static int launch_one(Engine* e, Plan* plan, const Launch& L, cudaStream_t st, b
   return GPUGA_OK;
 }
 
-// Folds the event pairs of the previous timed generation into the per-launch totals.
-int plan_collect_timing(Plan* plan) {
-  if (!plan->t_pending) return GPUGA_OK;
-  for (size_t k = 0; k < plan->launches.size(); ++k) {
-    GPUGA_CUDA(cudaEventSynchronize(plan->tev[2 * k + 1]));
-    float ms = 0.f;
-    GPUGA_CUDA(cudaEventElapsedTime(&ms, plan->tev[2 * k], plan->tev[2 * k + 1]));
-    plan->t_ms[k] += ms;
+}  // namespace
+
+int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSet* ls) {
+  std::map<LaunchKey, std::vector<ItemSpec>> groups;
+  std::map<LaunchKey, size_t> smem_need;
+  std::vector<int2> indmap;
+  ls->jobs.clear();
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    GPUGA_TRY(job_items(jobs[j].first, jobs[j].second->P, (int)j, groups, smem_need));
+    ls->jobs.push_back(make_job_view(jobs[j].first, jobs[j].second));
+    for (int p = 0; p < jobs[j].second->P; ++p) indmap.push_back(make_int2((int)j, p));
   }
-  plan->t_count += 1;
-  plan->t_pending = false;
+  std::vector<WorkItem> all;
+  ls->launches.clear();
+  for (auto& kv : groups) {
+    auto& v = kv.second;
+    std::stable_sort(v.begin(), v.end(), [](const ItemSpec& a, const ItemSpec& b) { return a.cost > b.cost; });
+    Launch L;
+    L.kind = kv.first.kind;
+    L.zclass = kv.first.zclass;
+    L.nmax = kv.first.nmax;
+    L.force = kv.first.force != 0;
+    L.smem = smem_need[kv.first];
+    L.count = (int)v.size();
+    L.first = all.size();
+    for (auto& t : v) {
+      all.push_back(t.w);
+      L.units += t.units;
+      L.flops += t.flops;
+      L.sfu += t.sfu;
+    }
+    ls->launches.push_back(L);
+  }
+  // longest launches first so that the side stream starts the big ones early
+  std::stable_sort(ls->launches.begin(), ls->launches.end(),
+                   [](const Launch& a, const Launch& b) { return a.flops > b.flops; });
+  ls->total_individuals = (int)indmap.size();
+  GPUGA_CUDA(cudaMalloc(&ls->d_items, sizeof(WorkItem) * std::max<size_t>(all.size(), 1)));
+  GPUGA_CUDA(cudaMemcpy(ls->d_items, all.data(), sizeof(WorkItem) * all.size(), cudaMemcpyHostToDevice));
+  GPUGA_CUDA(cudaMalloc(&ls->d_indmap, sizeof(int2) * std::max<size_t>(indmap.size(), 1)));
+  GPUGA_CUDA(cudaMemcpy(ls->d_indmap, indmap.data(), sizeof(int2) * indmap.size(), cudaMemcpyHostToDevice));
+  GPUGA_CUDA(cudaMalloc(&ls->d_jobs, sizeof(JobView) * std::max<size_t>(ls->jobs.size(), 1)));
+  GPUGA_CUDA(cudaMallocHost(&ls->h_jobs, sizeof(JobView) * std::max<size_t>(ls->jobs.size(), 1)));
+  GPUGA_CUDA(cudaMemcpy(ls->d_jobs, ls->jobs.data(), sizeof(JobView) * ls->jobs.size(), cudaMemcpyHostToDevice));
+  GPUGA_CUDA(cudaStreamCreateWithFlags(&ls->side, cudaStreamNonBlocking));
+  GPUGA_CUDA(cudaEventCreateWithFlags(&ls->fork, cudaEventDisableTiming));
+  GPUGA_CUDA(cudaEventCreateWithFlags(&ls->join, cudaEventDisableTiming));
+  ls->tev.assign(2 * ls->launches.size(), nullptr);
+  for (auto& ev : ls->tev) GPUGA_CUDA(cudaEventCreate(&ev));
+  ls->t_ms.assign(ls->launches.size(), 0.0);
+  for (const Launch& L : ls->launches) GPUGA_TRY(launch_one(ls, L, nullptr, true));
   return GPUGA_OK;
 }
 
-// Enqueues one generation: decode, the batched force launches (energy/virial
-// items on `st`, force items on the plan's side stream), then the fitness fold.
-int batched_enqueue(Engine* e, Plan* plan, const float* d_pop, double* d_fitness, cudaStream_t st) {
-  const DevSet& d = e->d;
-  const int P = plan->P;
-  decode_population<<<(P + 127) / 128, 128, 0, st>>>(P, d.num_vars, d.potential_type, d.num_types, d_pop,
-                                                     e->d_pmin, e->d_pmax, plan->Pstride, plan->d_consts,
-                                                     plan->d_weights);
+int launchset_retarget(LaunchSet* ls, int job, const float* d_pop, double* d_fitness, float* fdump,
+                       cudaStream_t st) {
+  JobView& j = ls->jobs[job];
+  if (j.pop == d_pop && j.fitness == d_fitness && j.fdump == fdump) return GPUGA_OK;
+  j.pop = d_pop;
+  j.fitness = d_fitness;
+  j.fdump = fdump;
+  // staged through pinned memory; the previous copy has completed once the stream reached it
+  GPUGA_CUDA(cudaStreamSynchronize(st));
+  ls->h_jobs[job] = j;
+  GPUGA_CUDA(cudaMemcpyAsync(ls->d_jobs + job, ls->h_jobs + job, sizeof(JobView), cudaMemcpyHostToDevice, st));
+  return GPUGA_OK;
+}
+
+// Folds the event pairs of the previous timed generation into the per-launch totals.
+int launchset_collect_timing(LaunchSet* ls) {
+  if (!ls->t_pending) return GPUGA_OK;
+  for (size_t k = 0; k < ls->launches.size(); ++k) {
+    GPUGA_CUDA(cudaEventSynchronize(ls->tev[2 * k + 1]));
+    float ms = 0.f;
+    GPUGA_CUDA(cudaEventElapsedTime(&ms, ls->tev[2 * k], ls->tev[2 * k + 1]));
+    ls->t_ms[k] += ms;
+  }
+  ls->t_count += 1;
+  ls->t_pending = false;
+  return GPUGA_OK;
+}
+
+// One generation of every job of the set: decode, the batched launches
+// (energy/virial launches on `st`, force launches on the side stream), then
+// the fitness fold.
+int launchset_enqueue(LaunchSet* ls, cudaStream_t st) {
+  const int total = ls->total_individuals;
+  decode_jobs<<<(total + 127) / 128, 128, 0, st>>>(ls->d_jobs, ls->d_indmap, total);
   GPUGA_CUDA(cudaGetLastError());
   bool any_side = false;
-  for (const Launch& L : plan->launches)
+  for (const Launch& L : ls->launches)
     if (L.force) any_side = true;
   if (any_side) {
-    GPUGA_CUDA(cudaEventRecord(plan->fork, st));
-    GPUGA_CUDA(cudaStreamWaitEvent(plan->side, plan->fork, 0));
+    GPUGA_CUDA(cudaEventRecord(ls->fork, st));
+    GPUGA_CUDA(cudaStreamWaitEvent(ls->side, ls->fork, 0));
   }
-  GPUGA_TRY(plan_collect_timing(plan));
-  for (size_t k = 0; k < plan->launches.size(); ++k) {
-    const Launch& L = plan->launches[k];
-    cudaStream_t ls = L.force ? plan->side : st;
-    if (plan->timing) GPUGA_CUDA(cudaEventRecord(plan->tev[2 * k], ls));
-    GPUGA_TRY(launch_one(e, plan, L, ls, false));
-    if (plan->timing) GPUGA_CUDA(cudaEventRecord(plan->tev[2 * k + 1], ls));
+  GPUGA_TRY(launchset_collect_timing(ls));
+  for (size_t k = 0; k < ls->launches.size(); ++k) {
+    const Launch& L = ls->launches[k];
+    cudaStream_t s = L.force ? ls->side : st;
+    if (ls->timing) GPUGA_CUDA(cudaEventRecord(ls->tev[2 * k], s));
+    GPUGA_TRY(launch_one(ls, L, s, false));
+    if (ls->timing) GPUGA_CUDA(cudaEventRecord(ls->tev[2 * k + 1], s));
   }
-  plan->t_pending = plan->timing;
+  ls->t_pending = ls->timing;
   if (any_side) {
-    GPUGA_CUDA(cudaEventRecord(plan->join, plan->side));
-    GPUGA_CUDA(cudaStreamWaitEvent(st, plan->join, 0));
+    GPUGA_CUDA(cudaEventRecord(ls->join, ls->side));
+    GPUGA_CUDA(cudaStreamWaitEvent(st, ls->join, 0));
   }
-  fitness_reduce<<<(P + 3) / 4, 128, 0, st>>>(P, d.Nc, d.Nc_force, plan->d_res, d.E_ref, d.W_ref, d.norm_force,
-                                              d.norm_energy, d.norm_virial, d.w_force, d.w_energy, d.w_stress,
-                                              d_fitness, plan->d_comps);
+  fitness_jobs<<<(total + 3) / 4, 128, 0, st>>>(ls->d_jobs, ls->d_indmap, total);
   GPUGA_CUDA(cudaGetLastError());
+  return GPUGA_OK;
+}
+
+int plan_build(Engine* e, int P, Plan** out) {
+  const DevSet& d = e->d;
+  std::unique_ptr<Plan> plan(new Plan);
+  plan->P = P;
+  plan->Pstride = (P + 31) & ~31;
+  const int K = consts_per_individual(d);
+  GPUGA_TRY(e->alloc(&plan->d_consts, (size_t)K * plan->Pstride));
+  if (d.potential_type == 3) GPUGA_TRY(e->alloc(&plan->d_weights, (size_t)d.num_vars * plan->Pstride));
+  GPUGA_TRY(e->alloc(&plan->d_res, (size_t)P * d.Nc * kResK));
+  GPUGA_TRY(e->alloc(&plan->d_fitness, (size_t)P));
+  GPUGA_TRY(e->alloc(&plan->d_comps, (size_t)3 * P));
+  GPUGA_TRY(e->alloc(&plan->d_pop, (size_t)P * d.num_vars));
+  GPUGA_CUDA(cudaMallocHost(&plan->h_pop, sizeof(float) * (size_t)P * d.num_vars));
+  GPUGA_CUDA(cudaMallocHost(&plan->h_fit, sizeof(double) * 4 * (size_t)P));
+  plan->ls.reset(new LaunchSet);
+  GPUGA_TRY(launchset_build({{e, plan.get()}}, plan->ls.get()));
+  *out = plan.release();
   return GPUGA_OK;
 }
 

@@ -249,22 +249,23 @@ int gpuga_plan_info(gpuga_engine* h, int P, int* n_launches, double* per_launch,
   GPUGA_CUDA(cudaSetDevice(h->e->device));
   int s = plan_get(h->e, P, &plan);
   if (s != GPUGA_OK) return s;
-  s = plan_collect_timing(plan);
+  LaunchSet* ls = plan->ls.get();
+  s = launchset_collect_timing(ls);
   if (s != GPUGA_OK) return s;
-  const int n = (int)plan->launches.size();
+  const int n = (int)ls->launches.size();
   if (n_launches) *n_launches = n;
   if (per_launch) {
     for (int k = 0; k < n && k < cap; ++k) {
-      const Launch& L = plan->launches[k];
+      const Launch& L = ls->launches[k];
       double* o = per_launch + 8 * (size_t)k;
       o[0] = L.kind;
-      o[1] = L.zclass;
+      o[1] = L.kind == 2 ? L.nmax : L.zclass;
       o[2] = L.force ? 1 : 0;
       o[3] = L.count;
       o[4] = L.units;
       o[5] = L.flops;
       o[6] = L.sfu;
-      o[7] = plan->t_count ? plan->t_ms[k] / plan->t_count : 0.0;
+      o[7] = ls->t_count ? ls->t_ms[k] / ls->t_count : 0.0;
     }
   }
   return GPUGA_OK;
@@ -276,11 +277,12 @@ int gpuga_kernel_timing(gpuga_engine* h, int P, int enable) {
   GPUGA_CUDA(cudaSetDevice(h->e->device));
   int s = plan_get(h->e, P, &plan);
   if (s != GPUGA_OK) return s;
-  s = plan_collect_timing(plan);
+  LaunchSet* ls = plan->ls.get();
+  s = launchset_collect_timing(ls);
   if (s != GPUGA_OK) return s;
-  plan->timing = enable != 0;
-  std::fill(plan->t_ms.begin(), plan->t_ms.end(), 0.0);
-  plan->t_count = 0;
+  ls->timing = enable != 0;
+  std::fill(ls->t_ms.begin(), ls->t_ms.end(), 0.0);
+  ls->t_count = 0;
   return GPUGA_OK;
 }
 

@@ -11,18 +11,7 @@ namespace gpuga {
 
 Engine::~Engine() {
   if (device >= 0) cudaSetDevice(device);
-  for (auto& kv : plans) {
-    Plan* p = kv.second.get();
-    if (p->graph) cudaGraphExecDestroy(p->graph);
-    if (p->h_pop) cudaFreeHost(p->h_pop);
-    if (p->h_fit) cudaFreeHost(p->h_fit);
-    if (p->side) cudaStreamDestroy(p->side);
-    if (p->fork) cudaEventDestroy(p->fork);
-    if (p->join) cudaEventDestroy(p->join);
-    for (auto ev : p->tev)
-      if (ev) cudaEventDestroy(ev);
-  }
-  plans.clear();
+  plans.clear();  // graphs, pinned staging and launch sets
   for (void* ptr : allocations) cudaFree(ptr);
   if (p_out) cudaFree(p_out);
   if (stream) cudaStreamDestroy(stream);
@@ -144,7 +133,7 @@ int get_plan(Engine* e, int P, Plan** out) { return plan_get(e, P, out); }
 int enqueue_generation(Engine* e, Plan* plan, cudaStream_t st) {
   const size_t nbytes = sizeof(float) * (size_t)plan->P * e->d.num_vars;
   GPUGA_CUDA(cudaMemcpyAsync(plan->d_pop, plan->h_pop, nbytes, cudaMemcpyHostToDevice, st));
-  GPUGA_TRY(batched_enqueue(e, plan, plan->d_pop, plan->d_fitness, st));
+  GPUGA_TRY(launchset_enqueue(plan->ls.get(), st));
   GPUGA_CUDA(cudaMemcpyAsync(plan->h_fit, plan->d_fitness, sizeof(double) * plan->P, cudaMemcpyDeviceToHost, st));
   GPUGA_CUDA(cudaMemcpyAsync(plan->h_fit + plan->P, plan->d_comps, sizeof(double) * 3 * plan->P,
                              cudaMemcpyDeviceToHost, st));
@@ -154,9 +143,13 @@ int enqueue_generation(Engine* e, Plan* plan, cudaStream_t st) {
 int run_batched(Engine* e, int P, const float* pop01, double* fitness, double* comps) {
   Plan* plan = nullptr;
   GPUGA_TRY(get_plan(e, P, &plan));
-  memcpy(plan->h_pop, pop01, sizeof(float) * (size_t)P * e->d.num_vars);
   cudaStream_t st = e->stream;
-  const bool use_graph = e->opt.use_graph && !plan->dump && !plan->timing;
+  // the staged path reads the plan's own population / fitness buffers
+  GPUGA_TRY(launchset_retarget(plan->ls.get(), 0, plan->d_pop, plan->d_fitness,
+                               plan->dump ? plan->d_fdump : nullptr, st));
+  GPUGA_CUDA(cudaStreamSynchronize(st));
+  memcpy(plan->h_pop, pop01, sizeof(float) * (size_t)P * e->d.num_vars);
+  const bool use_graph = e->opt.use_graph && !plan->dump && !plan->ls->timing;
   if (use_graph) {
     if (!plan->graph) {
       cudaGraph_t g = nullptr;
@@ -201,12 +194,13 @@ int engine_fitness(Engine* e, int path, int P, const float* pop01, double* fitne
   }
 }
 
-// C-ABI helpers that need the plan internals.
+// Batched path on caller-owned device buffers, enqueued on the caller's stream.
 int engine_fitness_device(Engine* e, int P, const float* d_pop, double* d_fitness, cudaStream_t st) {
   GPUGA_CUDA(cudaSetDevice(e->device));
   Plan* plan = nullptr;
   GPUGA_TRY(get_plan(e, P, &plan));
-  return batched_enqueue(e, plan, d_pop, d_fitness, st);
+  GPUGA_TRY(launchset_retarget(plan->ls.get(), 0, d_pop, d_fitness, nullptr, st));
+  return launchset_enqueue(plan->ls.get(), st);
 }
 
 int engine_last_results(Engine* e, int P, double* energy, double* virial, double* force_sq) {

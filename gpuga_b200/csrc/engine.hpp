@@ -55,33 +55,96 @@ struct DevSet {
   float w_force = 0, w_energy = 0, w_stress = 0;
 };
 
-// One CTA of a batched launch: config c for individuals [p0, p0 + G).
+// One CTA of a batched launch: configuration `config` of job `job` for
+// individuals [p0, p0 + G).
 struct WorkItem {
   int config;
   int p0;
-  int G;      // individuals per item (power of two <= 32); lanes = G individuals x (32/G) atoms
-  int flags;  // bit0: force configuration
+  int G;    // individuals per item (power of two <= 32); lanes = G individuals x (32/G) atoms
+  int job;  // row of the launch set's job table
+};
+
+// Read-only training-set view the batched kernels use.
+struct DevView {
+  int Nc, N, N_force;
+  const int* Na;
+  const int* Na_sum;
+  const int* NN;
+  const int* off;
+  const int* half_off;
+  const int* trip_off;
+  const int* rev;
+  const uint8_t* ptype;
+  const float4* g32;
+  const float4* gri;
+  const float* cosm;
+  const float* force_ref;
+};
+
+struct NNTaper {
+  float r1, r2, pf;
+  int consistent;
+};
+
+// One row of a launch set's job table: a training set, a population and the
+// buffers of its evaluation.  Several jobs share the same launches.
+struct JobView {
+  DevView v;
+  int potential_type, num_types, num_neurons, num_vars, P, Pstride, Nc_force;
+  NNTaper tp;
+  const float* pop;      // [P][num_vars] in [0,1]
+  const float* pmin;
+  const float* pmax;
+  float* consts;         // [K][Pstride]
+  float* weights;        // NN2B [num_vars][Pstride]
+  double* res;           // [P][Nc][kResK]
+  float* fdump;          // optional [P][3][N_force]
+  const double* E_ref;
+  const double* W_ref;
+  double nF, nE, nW;
+  float wF, wE, wW;
+  double* fitness;       // [P]
+  double* comps;         // [P][3]
 };
 
 struct Launch {
   int kind = 0;        // 0 Tersoff, 1 RI, 2 NN2B
-  double units = 0;    // (individual, atom) pairs per launch
-  double flops = 0;    // algorithmic FP32 flops per launch (FMA = 2)
-  double sfu = 0;      // transcendental calls per launch
   int zclass = 4;      // Tersoff register-array size
+  int nmax = 0;        // NN2B register-array size
   bool force = false;  // force items (gather pass) vs energy/virial items
   size_t smem = 0;
   int count = 0;
-  WorkItem* d_items = nullptr;  // slice of the engine's item buffer
+  size_t first = 0;    // offset of the launch's items in the set's item array
+  double units = 0;    // (individual, atom) pairs per launch
+  double flops = 0;    // algorithmic FP32 flops per launch (FMA = 2)
+  double sfu = 0;      // transcendental calls per launch
 };
 
+// Launches of one generation over one or more jobs (a job table on the device).
+struct LaunchSet {
+  std::vector<Launch> launches;
+  std::vector<JobView> jobs;   // host copy of the table
+  JobView* d_jobs = nullptr;
+  JobView* h_jobs = nullptr;   // pinned staging for table updates
+  WorkItem* d_items = nullptr;
+  int2* d_indmap = nullptr;    // global individual -> (job, p)
+  int total_individuals = 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  bool timing = false;               // event pair around every launch (eager launches)
+  std::vector<cudaEvent_t> tev;      // 2 per launch
+  std::vector<double> t_ms;          // accumulated device time per launch
+  int t_count = 0;
+  bool t_pending = false;
+  ~LaunchSet();
+};
+
+// Per (engine, population size) buffers plus the engine's own launch set.
 struct Plan {
   int P = 0;
-  std::vector<Launch> launches;
-  WorkItem* d_items = nullptr;
-  float* d_consts = nullptr;   // [kMaxConsts][Pstride] per-individual constants
-  float* d_weights = nullptr;  // NN2B weights [num_vars][Pstride]
   int Pstride = 0;
+  float* d_consts = nullptr;   // [K][Pstride] per-individual constants
+  float* d_weights = nullptr;  // NN2B weights [num_vars][Pstride]
   double* d_res = nullptr;     // [P][Nc][kResK]
   double* d_fitness = nullptr; // [P]
   double* d_comps = nullptr;   // [P][3]
@@ -91,13 +154,8 @@ struct Plan {
   float* d_fdump = nullptr;    // optional per-atom forces of force configs [P][3][N_force]
   bool dump = false;           // pass d_fdump to the kernels (eager launches only)
   cudaGraphExec_t graph = nullptr;
-  cudaStream_t side = nullptr;
-  bool timing = false;                // record an event pair around every launch (eager launches)
-  std::vector<cudaEvent_t> tev;       // 2 per launch
-  std::vector<double> t_ms;           // accumulated device time per launch
-  int t_count = 0;                    // generations accumulated
-  bool t_pending = false;
-  cudaEvent_t fork = nullptr, join = nullptr;
+  std::unique_ptr<LaunchSet> ls;
+  ~Plan();
 };
 
 struct Engine {
@@ -138,11 +196,35 @@ int build_geometry(Engine* e);
 int neighbor_reference_layout(int Nc, int N, int max_Na, const int* Na, const int* Na_sum, const float* r,
                               const float* h, float cutoff, int* NN, int* NL, cudaStream_t st);
 
+int ref_layout_geometry(int Nc, int N, const int* Na, const int* Na_sum, const float* h, const float* r,
+                        const int* NN, const int* NL, double4* g64, int* rev, cudaStream_t st);
+
+// The reference's Potential interface on caller-owned device arrays in the
+// reference layouts (potential.cuh:22-41); scratch is supplied by the caller.
+struct RefPotentialScratch {
+  double4* g64;  // [max_Na * N]
+  int* rev;      // [max_Na * N]
+  float* f5;     // [5 * max_Na * N]: b, b', f_ij x/y/z
+  float* w;      // NN2B weights [num_vars]
+};
+size_t ref_potential_scratch_bytes(int potential_type, int num_neurons, int N, int max_Na);
+int ref_potential_find_force(int potential_type, int num_neurons, const float* params, const PotentialSpec& nn_opts,
+                             int Nc, int N, const int* Na, const int* Na_sum, int max_Na, const int* type,
+                             const float* h, const int* NN, const int* NL, const float* r, float* f, float* virial,
+                             float* pe, const RefPotentialScratch& s, cudaStream_t st);
+
 // batched.cu
 int plan_build(Engine* e, int P, Plan** out);
-int batched_enqueue(Engine* e, Plan* plan, const float* d_pop, double* d_fitness, cudaStream_t st);
 int consts_per_individual(const DevSet& d);
-int plan_collect_timing(Plan* plan);
+JobView make_job_view(const Engine* e, const Plan* plan);
+// Builds the shared launches of the given jobs (one engine + plan each).
+int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSet* ls);
+// Enqueues one generation of every job of the set on `st` (force launches on a side stream).
+int launchset_enqueue(LaunchSet* ls, cudaStream_t st);
+int launchset_collect_timing(LaunchSet* ls);
+// Points job row `job` at new population / fitness / force-dump buffers (enqueued on `st`).
+int launchset_retarget(LaunchSet* ls, int job, const float* d_pop, double* d_fitness, float* fdump,
+                       cudaStream_t st);
 int plan_get(Engine* e, int P, Plan** out);
 
 // plain.cu

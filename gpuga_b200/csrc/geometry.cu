@@ -183,6 +183,52 @@ __global__ void triplet_cosines(int N, const int* __restrict__ off, const int* _
   }
 }
 
+// Bond geometry for lists in the reference layout NL[k*N + i]: the FP32 rule
+// picks the image, the vector is then evaluated in FP64; rev holds the slot of
+// the reverse bond (slot 0 of the neighbor when absent, minimal_tersoff.cu:368).
+template <int MODE>
+__global__ void ref_layout_bonds(int N, const int* __restrict__ Na, const int* __restrict__ Na_sum,
+                                 const float* __restrict__ box, const float* __restrict__ r,
+                                 const int* __restrict__ NN, const int* __restrict__ NL, double4* __restrict__ g64,
+                                 int* __restrict__ rev) {
+  const int c = blockIdx.x;
+  const int n_begin = Na_sum[c], n_end = n_begin + Na[c];
+  const float* h = box + 18 * (size_t)c;
+  float hh[18];
+#pragma unroll
+  for (int k = 0; k < 18; ++k) hh[k] = h[k];
+  for (int i = n_begin + threadIdx.x; i < n_end; i += blockDim.x) {
+    const float x1 = r[i], y1 = r[i + N], z1 = r[i + 2 * (size_t)N];
+    for (int k = 0; k < NN[i]; ++k) {
+      const size_t slot = (size_t)k * N + i;
+      const int j = NL[slot];
+      float x12 = __fsub_rn(r[j], x1), y12 = __fsub_rn(r[j + N], y1), z12 = __fsub_rn(r[j + 2 * (size_t)N], z1);
+      float ix, iy, iz;
+      mic32<MODE>(hh, x12, y12, z12, ix, iy, iz);
+      double dx = (double)r[j] - (double)x1, dy = (double)r[j + N] - (double)y1,
+             dz = (double)r[j + 2 * (size_t)N] - (double)z1;
+      dx -= (double)hh[0] * ix + (double)hh[1] * iy + (double)hh[2] * iz;
+      dy -= (double)hh[3] * ix + (double)hh[4] * iy + (double)hh[5] * iz;
+      dz -= (double)hh[6] * ix + (double)hh[7] * iy + (double)hh[8] * iz;
+      g64[slot] = make_double4(dx, dy, dz, sqrt(dx * dx + dy * dy + dz * dz));
+      int rs = j;
+      for (int kk = 0; kk < NN[j]; ++kk)
+        if (NL[(size_t)kk * N + j] == i) {
+          rs = kk * N + j;
+          break;
+        }
+      rev[slot] = rs;
+    }
+  }
+}
+
+int ref_layout_geometry(int Nc, int N, const int* Na, const int* Na_sum, const float* h, const float* r,
+                        const int* NN, const int* NL, double4* g64, int* rev, cudaStream_t st) {
+  ref_layout_bonds<kMicMode><<<Nc, 128, 0, st>>>(N, Na, Na_sum, h, r, NN, NL, g64, rev);
+  GPUGA_CUDA(cudaGetLastError());
+  return GPUGA_OK;
+}
+
 int neighbor_reference_layout(int Nc, int N, int max_Na, const int* Na, const int* Na_sum, const float* r,
                               const float* h, float cutoff, int* NN, int* NL, cudaStream_t st) {
   (void)max_Na;

@@ -46,6 +46,25 @@ __device__ __forceinline__ void fcut(T r1, T r2, T pf, T d, T& fc, T& fcp) {
   }
 }
 
+// Neighbor-list layouts: the engine's CSR lists, or the reference's
+// NL[k*N + i] (neighbor.cu:61) for the drop-in Potential entry points.  A bond
+// slot indexes the per-bond arrays (geometry, reverse slot, scratch).
+struct CsrLayout {
+  const int* off;
+  const int* nbr;
+  __device__ __forceinline__ int count(int i) const { return off[i + 1] - off[i]; }
+  __device__ __forceinline__ int slot(int i, int k) const { return off[i] + k; }
+  __device__ __forceinline__ int nb(int i, int k) const { return nbr[off[i] + k]; }
+};
+struct RefLayout {
+  int N;
+  const int* NN;
+  const int* NL;
+  __device__ __forceinline__ int count(int i) const { return NN[i]; }
+  __device__ __forceinline__ int slot(int i, int k) const { return k * N + i; }
+  __device__ __forceinline__ int nb(int i, int k) const { return NL[(size_t)k * N + i]; }
+};
+
 template <class T>
 __device__ __forceinline__ void bond(const double4* g, int b, T& x, T& y, T& z, T& d) {
   const double4 q = g[b];
@@ -56,17 +75,21 @@ __device__ __forceinline__ void bond(const double4* g, int b, T& x, T& y, T& z, 
 }
 
 // step 1 (minimal_tersoff.cu:122-188): bond orders
-template <class T>
-__global__ void p_tersoff1(int N, const int* __restrict__ off, const int* __restrict__ nbr,
-                           const double4* __restrict__ g, PT<T> P, T* __restrict__ b, T* __restrict__ bp) {
+template <class T, class Lay>
+__global__ void p_tersoff1(int N, Lay L, const double4* __restrict__ g, PT<T> P, T* __restrict__ b,
+                           T* __restrict__ bp) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  for (int i1 = off[i]; i1 < off[i + 1]; ++i1) {
+  const int Z = L.count(i);
+  for (int k1 = 0; k1 < Z; ++k1) {
+    const int i1 = L.slot(i, k1);
+    const int n2 = L.nb(i, k1);
     T x12, y12, z12, d12;
     bond(g, i1, x12, y12, z12, d12);
     T zeta = 0;
-    for (int i2 = off[i]; i2 < off[i + 1]; ++i2) {
-      if (nbr[i2] == nbr[i1]) continue;
+    for (int k2 = 0; k2 < Z; ++k2) {
+      const int i2 = L.slot(i, k2);
+      if (L.nb(i, k2) == n2) continue;
       T x13, y13, z13, d13;
       bond(g, i2, x13, y13, z13, d13);
       const T cs = (x12 * x13 + y12 * y13 + z12 * z13) / (d12 * d13);
@@ -88,17 +111,19 @@ __global__ void p_tersoff1(int N, const int* __restrict__ off, const int* __rest
 }
 
 // step 2 (minimal_tersoff.cu:191-316): partial forces and site energies
-template <class T>
-__global__ void p_tersoff2(int N, int num_types, const int* __restrict__ type, const int* __restrict__ off,
-                           const int* __restrict__ nbr, const double4* __restrict__ g, PT<T> P,
-                           const T* __restrict__ b, const T* __restrict__ bp, T* __restrict__ pe,
-                           T* __restrict__ fxs, T* __restrict__ fys, T* __restrict__ fzs) {
+template <class T, class Lay>
+__global__ void p_tersoff2(int N, int num_types, const int* __restrict__ type, Lay L,
+                           const double4* __restrict__ g, PT<T> P, const T* __restrict__ b,
+                           const T* __restrict__ bp, T* __restrict__ pe, T* __restrict__ fxs,
+                           T* __restrict__ fys, T* __restrict__ fzs) {
   const int n1 = blockIdx.x * blockDim.x + threadIdx.x;
   if (n1 >= N) return;
   const int type1 = type[n1];
+  const int Z = L.count(n1);
   T pot = 0;
-  for (int i1 = off[n1]; i1 < off[n1 + 1]; ++i1) {
-    const int n2 = nbr[i1];
+  for (int k1 = 0; k1 < Z; ++k1) {
+    const int i1 = L.slot(n1, k1);
+    const int n2 = L.nb(n1, k1);
     const int s12 = (num_types == 2 && type1 != type[n2]) ? 1 : 0;
     T x12, y12, z12, d12;
     bond(g, i1, x12, y12, z12, d12);
@@ -115,8 +140,9 @@ __global__ void p_tersoff2(int N, int num_types, const int* __restrict__ type, c
     T f12x = x12 * factor3 * T(0.5), f12y = y12 * factor3 * T(0.5), f12z = z12 * factor3 * T(0.5);
     pot += fc12 * (fr12 - b12 * fa12) * T(0.5);
     const T bp12 = bp[i1];
-    for (int i2 = off[n1]; i2 < off[n1 + 1]; ++i2) {
-      const int n3 = nbr[i2];
+    for (int k2 = 0; k2 < Z; ++k2) {
+      const int i2 = L.slot(n1, k2);
+      const int n3 = L.nb(n1, k2);
       if (n3 == n2) continue;
       const int s13 = (num_types == 2 && type1 != type[n3]) ? 1 : 0;
       T x13, y13, z13, d13;
@@ -148,14 +174,16 @@ __global__ void p_tersoff2(int N, int num_types, const int* __restrict__ type, c
 }
 
 // step 3 (minimal_tersoff.cu:318-405): force gather and per-atom virial
-template <class T>
-__global__ void p_tersoff3(int N, const int* __restrict__ off, const int* __restrict__ rev,
-                           const double4* __restrict__ g, const T* __restrict__ fxs, const T* __restrict__ fys,
-                           const T* __restrict__ fzs, T* __restrict__ F, T* __restrict__ W) {
+template <class T, class Lay>
+__global__ void p_tersoff3(int N, Lay L, const int* __restrict__ rev, const double4* __restrict__ g,
+                           const T* __restrict__ fxs, const T* __restrict__ fys, const T* __restrict__ fzs,
+                           T* __restrict__ F, T* __restrict__ W) {
   const int n1 = blockIdx.x * blockDim.x + threadIdx.x;
   if (n1 >= N) return;
   T sfx = 0, sfy = 0, sfz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vyz = 0, vzx = 0;
-  for (int i1 = off[n1]; i1 < off[n1 + 1]; ++i1) {
+  const int Z = L.count(n1);
+  for (int k1 = 0; k1 < Z; ++k1) {
+    const int i1 = L.slot(n1, k1);
     T x12, y12, z12, d12;
     bond(g, i1, x12, y12, z12, d12);
     const int r = rev[i1];
@@ -226,19 +254,20 @@ __device__ void nn_p2f2(const T* __restrict__ w, int n, T d, T& p2, T& f2) {
 }
 
 // ri.cu:112-189 / nn2b.cu:94-173
-template <class T>
-__global__ void p_pair(int N, int kind, const int* __restrict__ type, const int* __restrict__ off,
-                       const int* __restrict__ nbr, const double4* __restrict__ g, PR<T> q,
+template <class T, class Lay>
+__global__ void p_pair(int N, int kind, const int* __restrict__ type, Lay L, const double4* __restrict__ g, PR<T> q,
                        const T* __restrict__ w, PN nn, T* __restrict__ F, T* __restrict__ W, T* __restrict__ pe) {
   const int n1 = blockIdx.x * blockDim.x + threadIdx.x;
   if (n1 >= N) return;
   T e = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vyz = 0, vzx = 0;
-  for (int i1 = off[n1]; i1 < off[n1 + 1]; ++i1) {
+  const int Z = L.count(n1);
+  for (int k1 = 0; k1 < Z; ++k1) {
+    const int i1 = L.slot(n1, k1);
     T x12, y12, z12, d12;
     bond(g, i1, x12, y12, z12, d12);
     T p2, f2;
     if (kind == 0) {
-      ri_p2f2(q, type[n1] + type[nbr[i1]], d12, p2, f2);
+      ri_p2f2(q, type[n1] + type[L.nb(n1, k1)], d12, p2, f2);
     } else {
       nn_p2f2(w, nn.n, d12, p2, f2);
       T fc, fcp;
@@ -425,10 +454,10 @@ int enqueue_force(Engine* e, const float* params, const Scratch<T>& s, cudaStrea
   const int N = d.N, grid = (N + 127) / 128;
   if (d.potential_type == 1 || d.potential_type == 2) {
     const PT<T> P = tersoff_consts<T>(params, d.num_types);
-    p_tersoff1<T><<<grid, 128, 0, st>>>(N, d.off, d.nbr, d.g64, P, s.b, s.bp);
-    p_tersoff2<T><<<grid, 128, 0, st>>>(N, d.num_types, d.type, d.off, d.nbr, d.g64, P, s.b, s.bp, s.pe, s.fx,
-                                        s.fy, s.fz);
-    p_tersoff3<T><<<grid, 128, 0, st>>>(N, d.off, d.rev, d.g64, s.fx, s.fy, s.fz, s.F, s.W);
+    const CsrLayout L{d.off, d.nbr};
+    p_tersoff1<T><<<grid, 128, 0, st>>>(N, L, d.g64, P, s.b, s.bp);
+    p_tersoff2<T><<<grid, 128, 0, st>>>(N, d.num_types, d.type, L, d.g64, P, s.b, s.bp, s.pe, s.fx, s.fy, s.fz);
+    p_tersoff3<T><<<grid, 128, 0, st>>>(N, L, d.rev, d.g64, s.fx, s.fy, s.fz, s.F, s.W);
   } else {
     PR<T> q{};
     PN nn{d.num_neurons, e->spec.nn_r1, e->spec.nn_r2, M_PI / ((double)e->spec.nn_r2 - e->spec.nn_r1),
@@ -445,8 +474,8 @@ int enqueue_force(Engine* e, const float* params, const Scratch<T>& s, cudaStrea
       GPUGA_CUDA(cudaMemcpyAsync(s.w, w.data(), sizeof(T) * d.num_vars, cudaMemcpyHostToDevice, st));
       GPUGA_CUDA(cudaStreamSynchronize(st));  // w is a stack buffer
     }
-    p_pair<T><<<grid, 128, 0, st>>>(N, d.potential_type == 0 ? 0 : 1, d.type, d.off, d.nbr, d.g64, q, s.w, nn,
-                                    s.F, s.W, s.pe);
+    p_pair<T><<<grid, 128, 0, st>>>(N, d.potential_type == 0 ? 0 : 1, d.type, CsrLayout{d.off, d.nbr}, d.g64, q,
+                                    s.w, nn, s.F, s.W, s.pe);
   }
   GPUGA_CUDA(cudaGetLastError());
   return GPUGA_OK;
@@ -518,10 +547,11 @@ int plain_find_force64(Engine* e, const double* params, double* F, double* W, do
     P.R2 = params[8 + off];
     P.PF = M_PI / (P.R2 - P.R1);
     P.MHON = -0.5 / P.EN;
-    p_tersoff1<double><<<grid, 128, 0, st>>>(N, d.off, d.nbr, d.g64, P, s.b, s.bp);
-    p_tersoff2<double><<<grid, 128, 0, st>>>(N, d.num_types, d.type, d.off, d.nbr, d.g64, P, s.b, s.bp, s.pe,
-                                             s.fx, s.fy, s.fz);
-    p_tersoff3<double><<<grid, 128, 0, st>>>(N, d.off, d.rev, d.g64, s.fx, s.fy, s.fz, s.F, s.W);
+    const CsrLayout L{d.off, d.nbr};
+    p_tersoff1<double><<<grid, 128, 0, st>>>(N, L, d.g64, P, s.b, s.bp);
+    p_tersoff2<double><<<grid, 128, 0, st>>>(N, d.num_types, d.type, L, d.g64, P, s.b, s.bp, s.pe, s.fx, s.fy,
+                                             s.fz);
+    p_tersoff3<double><<<grid, 128, 0, st>>>(N, L, d.rev, d.g64, s.fx, s.fy, s.fz, s.F, s.W);
   } else {
     PR<double> q{};
     PN nn{d.num_neurons, e->spec.nn_r1, e->spec.nn_r2, M_PI / ((double)e->spec.nn_r2 - e->spec.nn_r1),
@@ -551,8 +581,8 @@ int plain_find_force64(Engine* e, const double* params, double* F, double* W, do
       }
       GPUGA_CUDA(cudaMemcpyAsync(s.w, params, sizeof(double) * d.num_vars, cudaMemcpyHostToDevice, st));
     }
-    p_pair<double><<<grid, 128, 0, st>>>(N, d.potential_type == 0 ? 0 : 1, d.type, d.off, d.nbr, d.g64, q, s.w,
-                                         nn, s.F, s.W, s.pe);
+    p_pair<double><<<grid, 128, 0, st>>>(N, d.potential_type == 0 ? 0 : 1, d.type, CsrLayout{d.off, d.nbr}, d.g64,
+                                         q, s.w, nn, s.F, s.W, s.pe);
   }
   GPUGA_CUDA(cudaGetLastError());
   if (F) GPUGA_CUDA(cudaMemcpyAsync(F, s.F, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st));
@@ -572,6 +602,61 @@ int plain_find_force32(Engine* e, const float* params, float* F, float* W, float
   if (W) GPUGA_CUDA(cudaMemcpyAsync(W, s.W, sizeof(float) * 6 * N, cudaMemcpyDeviceToHost, st));
   if (pe) GPUGA_CUDA(cudaMemcpyAsync(pe, s.pe, sizeof(float) * N, cudaMemcpyDeviceToHost, st));
   GPUGA_CUDA(cudaStreamSynchronize(st));
+  return GPUGA_OK;
+}
+
+// --------------------------------------------------------------- reference-layout Potential
+size_t ref_potential_scratch_bytes(int potential_type, int num_neurons, int N, int max_Na) {
+  const size_t slots = (size_t)N * (size_t)max_Na;
+  const int nv = std::max(num_vars_for(potential_type, num_neurons), 1);
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  return up(slots * sizeof(double4)) + up(slots * sizeof(int)) + up(5 * slots * sizeof(float)) +
+         up((size_t)nv * sizeof(float));
+}
+
+// Potential::find_force (potential.cuh:28-40) in FP32 on the reference's
+// layouts: bond geometry from the FP32 image rule, then the three Tersoff steps
+// or the pair loop, all enqueued on `st`; nothing is allocated here.
+int ref_potential_find_force(int potential_type, int num_neurons, const float* params, const PotentialSpec& nn_opts,
+                             int Nc, int N, const int* Na, const int* Na_sum, int max_Na, const int* type,
+                             const float* h, const int* NN, const int* NL, const float* r, float* f, float* virial,
+                             float* pe, const RefPotentialScratch& s, cudaStream_t st) {
+  (void)max_Na;
+  GPUGA_TRY(ref_layout_geometry(Nc, N, Na, Na_sum, h, r, NN, NL, s.g64, s.rev, st));
+  const size_t slots = (size_t)N * (size_t)max_Na;
+  float* b = s.f5;
+  float* bp = s.f5 + slots;
+  float* fx = s.f5 + 2 * slots;
+  float* fy = s.f5 + 3 * slots;
+  float* fz = s.f5 + 4 * slots;
+  const RefLayout L{N, NN, NL};
+  const int grid = (N + 127) / 128;
+  if (potential_type == 1 || potential_type == 2) {
+    const int num_types = potential_type == 2 ? 2 : 1;
+    const PT<float> P = tersoff_consts<float>(params, num_types);
+    p_tersoff1<float><<<grid, 128, 0, st>>>(N, L, s.g64, P, b, bp);
+    p_tersoff2<float><<<grid, 128, 0, st>>>(N, num_types, type, L, s.g64, P, b, bp, pe, fx, fy, fz);
+    p_tersoff3<float><<<grid, 128, 0, st>>>(N, L, s.rev, s.g64, fx, fy, fz, f, virial);
+  } else if (potential_type == 0 || potential_type == 3) {
+    PR<float> q{};
+    PN nn{num_neurons, nn_opts.nn_r1, nn_opts.nn_r2, M_PI / ((double)nn_opts.nn_r2 - nn_opts.nn_r1),
+          nn_opts.nn_consistent};
+    if (potential_type == 0) {
+      q = ri_consts<float>(params);
+    } else {
+      if (num_neurons > 32) {
+        set_error("the NN2B Potential entry points support up to 32 neurons per layer.");
+        return GPUGA_ERR_UNSUPPORTED;
+      }
+      GPUGA_CUDA(cudaMemcpyAsync(s.w, params, sizeof(float) * num_vars_for(3, num_neurons), cudaMemcpyHostToDevice,
+                                 st));
+    }
+    p_pair<float><<<grid, 128, 0, st>>>(N, potential_type == 0 ? 0 : 1, type, L, s.g64, q, s.w, nn, f, virial, pe);
+  } else {
+    set_error("unsupported potential type %d.", potential_type);
+    return GPUGA_ERR_UNSUPPORTED;
+  }
+  GPUGA_CUDA(cudaGetLastError());
   return GPUGA_OK;
 }
 

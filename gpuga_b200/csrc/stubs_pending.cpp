@@ -9,14 +9,6 @@ extern "C" {
     set_error(#name " is not implemented yet.");   \
     return GPUGA_ERR_UNSUPPORTED;                  \
   }
-PENDING(gpuga_potential_create, int, int, gpuga_potential**)
-PENDING(gpuga_potential_initialize, gpuga_potential*, int, int)
-PENDING(gpuga_potential_update, gpuga_potential*, const float*, int)
-PENDING(gpuga_potential_find_force, gpuga_potential*, int, int, const int*, const int*, int, const int*,
-        const float*, const int*, const int*, const float*, float*, float*, float*, void*)
-PENDING(gpuga_potential_destroy, gpuga_potential*)
-PENDING(gpuga_neighbor_compute, int, int, int, const int*, const int*, const float*, const float*, float, int*,
-        int*, void*)
 PENDING(gpuga_server_create, int, double, int, gpuga_server**)
 PENDING(gpuga_server_submit, gpuga_server*, const char*, unsigned, int, int*)
 PENDING(gpuga_server_submit_engine, gpuga_server*, gpuga_engine*, int, int, float, int, unsigned, int*)
