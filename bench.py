@@ -52,6 +52,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-individuals", type=int, default=48)
+    ap.add_argument("--configs", type=int, default=None, help="override the workload's configuration count")
+    ap.add_argument("--population", type=int, default=None, help="override the workload's population size")
     return ap.parse_args()
 
 
@@ -171,10 +173,12 @@ def engine_opts(data, device):
     return kw
 
 
-def build_workload(workload: int, device: int):
+def build_workload(workload: int, device: int, Nc=None, P=None):
     """Synthetic set with teacher targets evaluated by the engine's own FP64 path."""
     from gpuga_b200 import Fitness, synth
-    data = synth.make(workload)
+    data = synth.make(workload, Nc=Nc)
+    if P:
+        data["ga"] = dict(data["ga"], population_size=P, parent_number=P // 2)
     with Fitness(arrays=data, **engine_opts(data, device)) as e0:
         def evaluate(_data, params):
             return e0.find_force64(params)
@@ -190,7 +194,7 @@ def run_ours(args, dist: Dist):
     dev = dist.local_rank
     torch.cuda.set_device(dev)
     L = _lib.load()
-    data, e = build_workload(args.workload, dev)
+    data, e = build_workload(args.workload, dev, args.configs, args.population)
     P = int(data["ga"]["population_size"])
     d = e.number_of_variables
     Natoms = e.N
@@ -332,7 +336,7 @@ def cpu_baseline(data, budget_s: float) -> dict:
     dt = time.perf_counter() - t0
     s.close()
     shutil.rmtree(d, ignore_errors=True)
-    return {"value": n * s.N / dt if False else n * int(data["Na"].sum()) / dt, "unit": UNIT,
+    return {"value": n * int(data["Na"].sum()) / dt, "unit": UNIT,
             "cores": oracle.num_threads(), "kind": "port",
             "sample": f"{n} individuals x full training set ({int(data['Na'].sum())} atoms), FP64 OpenMP oracle, "
                       f"{dt:.1f} s"}
@@ -346,7 +350,9 @@ def run_reference(args, dist: Dist):
     if not os.path.exists(probe):
         return {"impl": "reference", "unavailable": "oracle/_ref/ref_probe was not built (needs the reference sources)"}
     from gpuga_b200 import synth
-    data = synth.make(args.workload)
+    data = synth.make(args.workload, Nc=args.configs)
+    if args.population:
+        data["ga"] = dict(data["ga"], population_size=args.population)
     if args.workload == 4:
         return {"impl": "reference", "unavailable": "the reference NN2B holds at most 10 neurons (nn2b.cuh:27-33)"}
     data = synth.fill_targets(data, oracle_evaluator())
@@ -356,10 +362,11 @@ def run_reference(args, dist: Dist):
     r = subprocess.run([probe, "time", d, str(P), str(args.steps), str(max(args.warmup, 3)), "12345678"],
                        capture_output=True, text=True, timeout=3000)
     shutil.rmtree(d, ignore_errors=True)
-    line = [ln for ln in r.stdout.splitlines() if ln.startswith("REF_TIME ")]
+    # the reference's start-up banner may leave the last line unterminated (neighbor.cu:78-82)
+    line = [ln[ln.index("REF_TIME ") + len("REF_TIME "):] for ln in r.stdout.splitlines() if "REF_TIME " in ln]
     if r.returncode != 0 or not line:
         return {"impl": "reference", "unavailable": f"ref_probe failed (rc={r.returncode}): {r.stderr[-300:]}"}
-    rt = json.loads(line[0][len("REF_TIME "):])
+    rt = json.loads(line[0])
     ms = rt["ms"]
     value = P * N * len(ms) / (sum(ms) / 1e3)
     sample = (f"reference CUDA build (GPUGA src/*.cu unmodified, nvcc -O3 --use_fast_math sm_100a) "
@@ -380,7 +387,7 @@ def main():
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:
             return 0
-        res = run_reference(args, Dist.__new__(Dist) if False else _RankZero())
+        res = run_reference(args, _RankZero())
         print(json.dumps(res))
         return 0
     dist = Dist()

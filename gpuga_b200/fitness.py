@@ -154,6 +154,70 @@ class Fitness:
         return NN, NL
 
 
+class Server:
+    """Continuous-batching server: many fitting jobs, one GPU, shared launches (gpuga_server_*)."""
+
+    QUEUED, RUNNING, DONE, FAILED, CANCELLED = range(5)
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: float = 120e9, max_jobs: int = 32):
+        self._h = C.c_void_p()
+        check(_lib.load().gpuga_server_create(device, float(hbm_budget_bytes), max_jobs, C.byref(self._h)))
+
+    def submit(self, input_dir: str, seed: int = 12345678, generations: int = 0) -> int:
+        jid = C.c_int()
+        check(_lib.load().gpuga_server_submit(self._h, input_dir.encode(), seed, generations, C.byref(jid)))
+        return jid.value
+
+    def submit_engine(self, fitness: "Fitness", population_size: int, parent_number: int, mutation_rate: float,
+                      generations: int, seed: int = 12345678) -> int:
+        jid = C.c_int()
+        check(_lib.load().gpuga_server_submit_engine(self._h, fitness.handle, population_size, parent_number,
+                                                     mutation_rate, generations, seed, C.byref(jid)))
+        return jid.value
+
+    def poll(self, job_id: int):
+        """(status, generations done, generations total, state)."""
+        prog = np.zeros(3, np.int32)
+        st = _lib.load().gpuga_server_poll(self._h, job_id, _p(prog))
+        return st, int(prog[0]), int(prog[1]), int(prog[2])
+
+    def result(self, job_id: int, generations: int, num_vars: int):
+        best = np.zeros(generations, np.float32)
+        elite = np.zeros(num_vars, np.float32)
+        check(_lib.load().gpuga_server_result(self._h, job_id, _p(best), _p(elite)))
+        return best, elite
+
+    def cancel(self, job_id: int) -> None:
+        check(_lib.load().gpuga_server_cancel(self._h, job_id))
+
+    def drain(self, timeout_s: float = 0.0) -> int:
+        return _lib.load().gpuga_server_drain(self._h, float(timeout_s))
+
+    def stats(self) -> dict:
+        s = np.zeros(8)
+        check(_lib.load().gpuga_server_stats(self._h, _p(s)))
+        keys = ("batches", "jobs_finished", "p50_gen_ms", "p99_gen_ms", "evals_per_s", "device_bytes",
+                "peak_resident_jobs", "total_evals")
+        return dict(zip(keys, (float(v) for v in s)))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.load().gpuga_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 class GA:
     """GA of src/ga.cu driven by a Fitness (GA::GA + GA::compute one generation at a time)."""
 
