@@ -75,6 +75,7 @@ PROTOTYPES = {
     "gpuga_potential_update": (i32, [vp, vp, i32]),
     "gpuga_potential_find_force": (i32, [vp, i32, i32, vp, vp, i32] + [vp] * 9),
     "gpuga_potential_destroy": (i32, [vp]),
+    "gpuga_potential_find_force_noalloc": (i32, [i32, i32, vp, i32, i32, i32, vp, vp, i32] + [vp] * 9),
     "gpuga_neighbor_compute": (i32, [i32, i32, i32, vp, vp, vp, vp, C.c_float, vp, vp, vp]),
     "gpuga_server_create": (i32, [i32, C.c_double, i32, vp]),
     "gpuga_server_submit": (i32, [vp, C.c_char_p, C.c_uint, i32, vp]),

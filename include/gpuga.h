@@ -183,6 +183,19 @@ int gpuga_potential_find_force(gpuga_potential* p, int Nc, int N, const int* Na,
                                const int* type, const float* h, const int* NN, const int* NL, const float* r,
                                float* f, float* virial, float* pe, void* stream);
 int gpuga_potential_destroy(gpuga_potential* p);
+/* No counterpart in the reference.  Same computation as gpuga_potential_create + _update +
+ * _find_force in one call that allocates nothing, for callers that cannot call cudaMalloc when
+ * they need forces (a code that gives its whole device-memory budget to its own allocator, a
+ * plug-in host that forbids device allocation after initialisation).  The caller passes all
+ * inputs and outputs (device pointers, reference layouts); the scratch is a fixed 64 MiB array
+ * per device inside the library, so N * max_Na * 56 bytes (+ the NN2B weights) must fit in it,
+ * otherwise GPUGA_ERR_ARG.  The first call on a device looks up that array's address and should
+ * come before any stream capture.  All calls on a device share the array: calls whose GPU work
+ * overlaps race on it, so serialise them. */
+int gpuga_potential_find_force_noalloc(int potential_type, int num_neurons, const float* params, int num_params,
+                                       int Nc, int N, const int* Na, const int* Na_sum, int max_Na, const int* type,
+                                       const float* h, const int* NN, const int* NL, const float* r, float* f,
+                                       float* virial, float* pe, void* stream);
 /* Neighbor::compute (neighbor.cu:68-83) on device arrays: NN int[N], NL int[max_Na*N]. */
 int gpuga_neighbor_compute(int Nc, int N, int max_Na, const int* Na, const int* Na_sum, const float* r,
                            const float* h, float cutoff, int* NN, int* NL, void* stream);
