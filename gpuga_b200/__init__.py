@@ -6,6 +6,7 @@ include/gpuga.h); this package holds thin ctypes bindings that mirror the
 reference's Fitness / GA interfaces and the seeded synthetic workloads.
 """
 from ._lib import (PATH_BATCHED, PATH_PLAIN32, PATH_PLAIN64, GpugaError, load)  # noqa: F401
-from .fitness import GA, Fitness, options  # noqa: F401
+from .fitness import GA, Fitness, Server, options  # noqa: F401
 
-__all__ = ["Fitness", "GA", "options", "load", "GpugaError", "PATH_BATCHED", "PATH_PLAIN64", "PATH_PLAIN32"]
+__all__ = ["Fitness", "GA", "Server", "options", "load", "GpugaError", "PATH_BATCHED", "PATH_PLAIN64",
+           "PATH_PLAIN32"]
