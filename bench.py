@@ -54,6 +54,9 @@ def parse_args():
     ap.add_argument("--plain-individuals", type=int, default=48)
     ap.add_argument("--configs", type=int, default=None, help="override the workload's configuration count")
     ap.add_argument("--population", type=int, default=None, help="override the workload's population size")
+    ap.add_argument("--serving", action="store_true", help="serving benchmark (workload 5) instead")
+    ap.add_argument("--serving-jobs", type=int, default=32)
+    ap.add_argument("--serving-generations", type=int, default=20)
     return ap.parse_args()
 
 
@@ -381,8 +384,62 @@ def run_reference(args, dist: Dist):
             "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))}}
 
 
+# ----------------------------------------------------------------------------- serving
+def run_serving(args) -> dict:
+    """Continuous batching: 32 fitting jobs drawn from workloads 1-3 (20..500 configurations each)
+    arriving as a Poisson process (2 jobs/s) into a server with a 120 GB budget.  Reports the
+    aggregate evals/s, p50/p99 generation latency and the one-job-at-a-time plain-FP64 estimate."""
+    import random
+
+    from gpuga_b200 import PATH_PLAIN64, Fitness, Server, synth
+    rng = random.Random(5)
+    gens = args.serving_generations
+    jobs = []
+    plain_rate = {}
+    tmp = tempfile.mkdtemp(prefix="gpuga_serving_")
+    for k in range(args.serving_jobs):
+        cfg = rng.choice([1, 2, 3])
+        Nc = rng.randint(20, 500) if cfg != 1 else 20
+        data = synth.make(cfg, seed=100 + k, Nc=Nc)
+        with Fitness(arrays=data, **engine_opts(data, 0)) as e0:
+            data = synth.fill_targets(data, lambda _d, p, e0=e0: e0.find_force64(p))
+            key = (cfg, Nc)
+            if cfg not in plain_rate:  # plain FP64 one-individual-per-launch rate of this potential
+                pop = synth.population(data, 4, seed=1)
+                e0.compute(1, pop[:1], path=PATH_PLAIN64)
+                t0 = time.perf_counter()
+                e0.compute(4, pop, path=PATH_PLAIN64)
+                plain_rate[cfg] = 4 * e0.N / (time.perf_counter() - t0)
+        d = synth.write_dir(data, os.path.join(tmp, f"job{k}"))
+        P = int(data["ga"]["population_size"])
+        jobs.append((d, cfg, P, int(data["Na"].sum())))
+    with Server(device=0, hbm_budget_bytes=120e9, max_jobs=32) as srv:
+        t0 = time.perf_counter()
+        ids = []
+        for k, (d, cfg, P, N) in enumerate(jobs):
+            ids.append(srv.submit(d, seed=1000 + k, generations=gens))
+            time.sleep(rng.expovariate(2.0))
+        rc = srv.drain(3000)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    shutil.rmtree(tmp, ignore_errors=True)
+    total_units = sum(P * N * gens for _, _, P, N in jobs)
+    serial_plain_s = sum(P * N * gens / plain_rate[cfg] for _, cfg, P, N in jobs)
+    return {"metric": "serving: aggregate fitness evals/s (indiv x atoms), 32 concurrent jobs", "value": st["evals_per_s"],
+            "unit": UNIT, "n_gpus": 1, "jobs": len(jobs), "generations_per_job": gens, "status": rc,
+            "latency_ms": {"p50": st["p50_gen_ms"], "p99": st["p99_gen_ms"]}, "wall_s": wall,
+            "peak_resident_jobs": st["peak_resident_jobs"], "generation_batches": st["batches"],
+            "total_units": total_units, "arrivals": "Poisson, 2 jobs/s",
+            "one_at_a_time_plain_fp64_s_estimate": serial_plain_s,
+            "speedup_vs_one_at_a_time_plain_fp64": serial_plain_s / max(wall, 1e-9),
+            "data": "synthetic (workloads 1-3, 20-500 configurations, teacher targets)"}
+
+
 def main():
     args = parse_args()
+    if args.serving:
+        print(json.dumps(run_serving(args)))
+        return 0
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:

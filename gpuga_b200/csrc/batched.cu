@@ -96,8 +96,8 @@ __global__ void decode_jobs(const JobView* __restrict__ jobs, const int2* __rest
     const double v_rc = erfc(alpha * rc) / rc;
     const double dv_rc = -erfc(alpha * rc) / (rc * rc) - pif * exp(-alpha * alpha * rc * rc) / rc;
     put(RC_RC, rc);
-    put(RC_VRC, v_rc);
-    put(RC_DVRC, dv_rc);
+    put(RC_VRC, J.ri_fixed_rc ? 0.0 : v_rc);  // a common cutoff is folded into the bond terms
+    put(RC_DVRC, J.ri_fixed_rc ? 0.0 : dv_rc);
     const double d0 = par(11), al = par(12), r0 = par(13), s = par(14);
     put(RC_LR, sqrt(2.0 * s) * al);
     put(RC_LA, sqrt(2.0 / s) * al);
@@ -156,24 +156,41 @@ __device__ __forceinline__ void cutoff_fn(float r1, float r2, float pf, float d,
   }
 }
 
-// Block-wide fixed-order reduction of the per-lane accumulators into res[p][c][k].
+// WorkItem::G packs the individuals per item (bits 0-7), whether the item's
+// geometry is staged in shared memory (bit 8) and the byte size of the force
+// scratch that precedes the staged geometry, in 16-byte units (bits 9-23).
+__host__ __device__ __forceinline__ int item_G(const WorkItem& it) { return it.G & 0xff; }
+__host__ __device__ __forceinline__ bool item_staged(const WorkItem& it) { return (it.G >> 8) & 1; }
+__host__ __device__ __forceinline__ size_t item_fbytes(const WorkItem& it) { return (size_t)((it.G >> 9) & 0x7fff) * 16; }
+__host__ __device__ __forceinline__ int pack_G(int G, bool staged, size_t fbytes) {
+  return G | (staged ? 1 << 8 : 0) | (int)(((fbytes + 15) / 16) << 9);
+}
+
+// Fixed-order fold of per-lane partial sums held in shared memory as
+// red[k * blockDim.x + thread] into res[p][c][k]: lanes of the same individual
+// (one per warp and atom slot) are added in thread order.
+__device__ __forceinline__ void fold_item(const WorkItem& it, int P, int Nc, const double* red,
+                                          double* __restrict__ res) {
+  __syncthreads();
+  const int G = item_G(it), A = 32 / G, nw = blockDim.x >> 5;
+  for (int t = threadIdx.x; t < G * kResK; t += blockDim.x) {
+    const int gg = t % G, k = t / G;
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w)
+      for (int a = 0; a < A; ++a) s += red[(size_t)k * blockDim.x + w * 32 + a * G + gg];
+    const int p = it.p0 + gg;
+    if (p < P) res[((size_t)p * Nc + it.config) * kResK + k] = s;
+  }
+}
+
+// Same for partial sums held in registers (they are first written out).
 __device__ __forceinline__ void reduce_item(const WorkItem& it, int P, int Nc, double (&acc)[kResK],
                                             unsigned char* smem, double* __restrict__ res) {
   __syncthreads();
   double* red = reinterpret_cast<double*>(smem);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < kResK; ++k) red[(warp * 32 + lane) * kResK + k] = acc[k];
-  __syncthreads();
-  const int G = it.G, A = 32 / G;
-  for (int t = threadIdx.x; t < G * kResK; t += blockDim.x) {
-    const int gg = t % G, k = t / G;
-    double s = 0.0;
-    for (int w = 0; w < kWarps; ++w)
-      for (int a = 0; a < A; ++a) s += red[(w * 32 + a * G + gg) * kResK + k];
-    const int p = it.p0 + gg;
-    if (p < P) res[((size_t)p * Nc + it.config) * kResK + k] = s;
-  }
+  for (int k = 0; k < kResK; ++k) red[(size_t)k * blockDim.x + threadIdx.x] = acc[k];
+  fold_item(it, P, Nc, red, res);
 }
 
 // One atom of the minimal Tersoff potential (minimal_tersoff.cu:122-405) for
@@ -185,53 +202,101 @@ __device__ __forceinline__ void reduce_item(const WorkItem& it, int P, int Nc, d
 // the reference's f_ij (minimal_tersoff.cu:250-307) is
 //   f_ij = 1/2 [ (A'_j - fc'_j sum_k T_k g_jk - m_j sum_k q_jk cos_jk) u_j + m_j sum_k q_jk u_k ]
 // with q_jk = beta (cos_jk - h) (S_j fc_k + T_k) and m_j = -2 fc_j / d_j.
-template <int ZC, bool FORCE>
-__device__ __forceinline__ float tersoff_atom(const DevView& S, const TersoffC& C, int i, int Z, float* fsm,
-                                              int bond0, int G, int g, float (&v)[6]) {
-  const int b0 = S.off[i];
+// Geometry of one configuration as a CTA sees it: in shared memory when the
+// work item was staged, otherwise the global arrays offset to the
+// configuration's first atom / bond / triplet.  All indices are local.
+struct Geo {
+  const float4* g;     // [Bc] (unit vector, d)
+  const uint8_t* pt;   // [Bc] pair set
+  const float* cs;     // [Tc] cos(theta) blocks
+  const int* rev;      // [Bc] reverse bond (global numbering; subtract bond0)
+  const int* nn;       // [Na]
+  const int* boff;     // [Na] bond offset (global numbering; subtract bond0)
+  const int* toff;     // [Na] triplet offset (global numbering; subtract trip0)
+  int bond0, trip0;
+};
+
+// Copies configuration c's geometry into shared memory with all threads of
+// the CTA (independent vector loads, then one barrier).
+__device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int Na, bool force, unsigned char* base) {
+  const int bond0 = S.off[atom0], bond1 = S.off[atom0 + Na];
+  const int trip0 = S.trip_off[atom0], trip1 = S.trip_off[atom0 + Na];
+  const int Bc = bond1 - bond0, Tc = trip1 - trip0;
+  float4* sg = reinterpret_cast<float4*>(base);
+  float* scs = reinterpret_cast<float*>(sg + Bc);
+  int* snn = reinterpret_cast<int*>(scs + Tc);
+  int* sbo = snn + Na;
+  int* sto = sbo + Na;
+  int* srev = sto + Na;
+  uint8_t* spt = reinterpret_cast<uint8_t*>(srev + (force ? Bc : 0));
+  for (int k = threadIdx.x; k < Bc; k += blockDim.x) {
+    sg[k] = __ldg(&S.g32[bond0 + k]);
+    spt[k] = S.ptype[bond0 + k];
+    if (force) srev[k] = S.rev[bond0 + k];
+  }
+  for (int k = threadIdx.x; k < Tc; k += blockDim.x) scs[k] = __ldg(&S.cosm[trip0 + k]);
+  for (int k = threadIdx.x; k < Na; k += blockDim.x) {
+    snn[k] = S.NN[atom0 + k];
+    sbo[k] = S.off[atom0 + k];
+    sto[k] = S.trip_off[atom0 + k];
+  }
+  __syncthreads();
+  return Geo{sg, spt, scs, srev, snn, sbo, sto, bond0, trip0};
+}
+
+__device__ __forceinline__ size_t staged_bytes(int Na, int Bc, int Tc, bool force) {
+  return (size_t)Bc * 16 + (size_t)Tc * 4 + (size_t)Na * 12 + (force ? (size_t)Bc * 4 : 0) + (size_t)Bc;
+}
+
+template <int ZC, int NT, bool FORCE>
+__device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C, int il, float* fsm, int G, int g,
+                                              float (&v)[6]) {
+  const int Z = geo.nn[il];
+  const int b0 = geo.boff[il] - geo.bond0;  // local
   float ux[ZC], uy[ZC], uz[ZC], dd[ZC];
   int st[ZC];
 #pragma unroll
   for (int j = 0; j < ZC; ++j) {
+    st[j] = 0;
     if (j < Z) {
-      const float4 q = __ldg(&S.g32[b0 + j]);
+      const float4 q = geo.g[b0 + j];
       ux[j] = q.x;
       uy[j] = q.y;
       uz[j] = q.z;
       dd[j] = q.w;
-      st[j] = S.ptype[b0 + j];
+      if (NT == 2) st[j] = geo.pt[b0 + j];
     } else {
       ux[j] = uy[j] = uz[j] = 0.f;
       dd[j] = 1.0f;
-      st[j] = 0;
     }
   }
-  float fc[ZC], fcp[ZC], fr[ZC], fa[ZC], fcb[ZC];
+  // pass A: pair terms and cutoff of every bond
+  float fc[ZC], fcp[ZC], fr[ZC], fa[ZC];
 #pragma unroll
   for (int j = 0; j < ZC; ++j) {
-    fc[j] = fcp[j] = fr[j] = fa[j] = fcb[j] = 0.f;
+    fc[j] = fcp[j] = fr[j] = fa[j] = 0.f;
     if (j < Z) {
-      const int s = st[j];
+      const int s = NT == 2 ? st[j] : 0;
       const float t = dd[j] - (s ? C.r0[1] : C.r0[0]);
       fr[j] = (s ? C.cr[1] : C.cr[0]) * expf(-(s ? C.lr[1] : C.lr[0]) * t);
       fa[j] = (s ? C.ca[1] : C.ca[0]) * expf(-(s ? C.la[1] : C.la[0]) * t);
       cutoff_fn(C.r1, C.r2, C.pf, dd[j], fc[j], fcp[j]);
-      fcb[j] = fc[j] * C.beta;
     }
   }
-  const float* cs = S.cosm + S.trip_off[i];
-  float bb[ZC], Sb[ZC], Tb[ZC];
+  // pass B: bond order, site energy and the per-bond force scalars
+  const float* cs = geo.cs + (geo.toff[il] - geo.trip0);
+  float Ap[ZC], Sb[ZC], Tb[ZC];
+  float pe = 0.f;
 #pragma unroll
   for (int j = 0; j < ZC; ++j) {
-    bb[j] = 1.f;
-    Sb[j] = Tb[j] = 0.f;
+    Ap[j] = Sb[j] = Tb[j] = 0.f;
     if (j < Z) {
       float zeta = 0.f;
 #pragma unroll
       for (int k = 0; k < ZC; ++k) {
         if (k < Z && k != j) {
-          const float x = __ldg(cs + j * Z + k) - C.h;
-          zeta = fmaf(fcb[k], x * x, zeta);
+          const float x = cs[j * Z + k] - C.h;
+          zeta = fmaf(fc[k] * C.beta, x * x, zeta);
         }
       }
       float b = 1.f, bp = 0.f;
@@ -239,29 +304,28 @@ __device__ __forceinline__ float tersoff_atom(const DevView& S, const TersoffC& 
         const float zn = powf(zeta, C.en);
         const float opz = 1.0f + zn;
         b = powf(opz, C.mhon);
-        bp = -0.5f * b * zn / (opz * zeta);
+        bp = -0.5f * b * zn * __frcp_rn(opz * zeta);
       }
-      bb[j] = b;
+      const int s = NT == 2 ? st[j] : 0;
+      const float e = fr[j] - b * fa[j];
+      pe = fmaf(0.5f * fc[j], e, pe);
+      const float frp = -(s ? C.lr[1] : C.lr[0]) * fr[j];
+      const float fap = -(s ? C.la[1] : C.la[0]) * fa[j];
+      Ap[j] = fcp[j] * e + fc[j] * (frp - b * fap);
       Sb[j] = bp * fa[j];
       Tb[j] = Sb[j] * fc[j];
     }
   }
-  float pe = 0.f;
+  // pass C: three-body force terms
 #pragma unroll
   for (int j = 0; j < ZC; ++j) {
     if (j < Z) {
-      const int s = st[j];
-      const float e = fr[j] - bb[j] * fa[j];
-      pe = fmaf(0.5f * fc[j], e, pe);
-      const float frp = -(s ? C.lr[1] : C.lr[0]) * fr[j];
-      const float fap = -(s ? C.la[1] : C.la[0]) * fa[j];
-      const float Ap = fcp[j] * e + fc[j] * (frp - bb[j] * fap);
       float sumG = 0.f, accC = 0.f, Vx = 0.f, Vy = 0.f, Vz = 0.f;
       const float Sj = Sb[j];
 #pragma unroll
       for (int k = 0; k < ZC; ++k) {
         if (k < Z && k != j) {
-          const float cjk = __ldg(cs + j * Z + k);
+          const float cjk = cs[j * Z + k];
           const float bx = C.beta * (cjk - C.h);
           const float g = bx * (cjk - C.h);
           const float q = bx * fmaf(Sj, fc[k], Tb[k]);
@@ -272,14 +336,14 @@ __device__ __forceinline__ float tersoff_atom(const DevView& S, const TersoffC& 
           Vz = fmaf(q, uz[k], Vz);
         }
       }
-      const float m = -2.0f * fc[j] / dd[j];
-      const float cu = 0.5f * (Ap - fcp[j] * sumG - m * accC);
+      const float m = -2.0f * fc[j] * __frcp_rn(dd[j]);
+      const float cu = 0.5f * (Ap[j] - fcp[j] * sumG - m * accC);
       const float cv = 0.5f * m;
       const float fx = fmaf(cu, ux[j], cv * Vx);
       const float fy = fmaf(cu, uy[j], cv * Vy);
       const float fz = fmaf(cu, uz[j], cv * Vz);
       if (FORCE) {
-        const int bl = b0 + j - bond0;
+        const int bl = b0 + j;
         fsm[(bl * 3 + 0) * G + g] = fx;
         fsm[(bl * 3 + 1) * G + g] = fy;
         fsm[(bl * 3 + 2) * G + g] = fz;
@@ -297,10 +361,15 @@ __device__ __forceinline__ float tersoff_atom(const DevView& S, const TersoffC& 
   return pe;
 }
 
-template <int ZC, bool FORCE>
-__global__ void __launch_bounds__(kBlock) tersoff_batched(const JobView* __restrict__ jobs,
-                                                          const WorkItem* __restrict__ items) {
+// Energy/virial items (FORCE = false) keep their FP64 per-lane sums in shared
+// memory (red[k][thread]) to save registers; a staged item's geometry follows
+// that region.  Force items put the f_ij scratch first, the staged geometry
+// after it, and reuse the start of shared memory for the final fold.
+template <int ZC, int NT, bool FORCE, int BLK>
+__global__ void __launch_bounds__(BLK) tersoff_batched(const JobView* __restrict__ jobs,
+                                                       const WorkItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int NW = BLK / 32;
   const WorkItem it = items[blockIdx.x];
   const JobView& J = jobs[it.job];
   const DevView S = J.v;
@@ -308,7 +377,7 @@ __global__ void __launch_bounds__(kBlock) tersoff_batched(const JobView* __restr
   double* __restrict__ res = J.res;
   float* __restrict__ fdump = J.fdump;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int G = it.G, A = 32 / G;
+  const int G = item_G(it), A = 32 / G;
   const int g = lane & (G - 1), aslot = lane / G;
   const int p = it.p0 + g;
   const Consts kc{J.consts, J.Pstride, p < P ? p : it.p0};
@@ -317,69 +386,108 @@ __global__ void __launch_bounds__(kBlock) tersoff_batched(const JobView* __restr
   const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
   const int bond0 = S.off[atom0];
   float* fsm = reinterpret_cast<float*>(smem);
-  double acc[kResK];
+  double* red = reinterpret_cast<double*>(smem);
+  const size_t front = FORCE ? item_fbytes(it) : (size_t)BLK * kResK * sizeof(double);
+  if (!FORCE) {
 #pragma unroll
-  for (int k = 0; k < kResK; ++k) acc[k] = 0.0;
-
-  for (int base = warp * A; base < Na; base += kWarps * A) {
+    for (int k = 0; k < 7; ++k) red[k * BLK + threadIdx.x] = 0.0;
+  }
+  const Geo geo = item_staged(it)
+                      ? stage_geometry(S, atom0, Na, FORCE, smem + front)
+                      : Geo{S.g32 + bond0, S.ptype + bond0, S.cosm + S.trip_off[atom0], S.rev + bond0,
+                            S.NN + atom0, S.off + atom0, S.trip_off + atom0, bond0, S.trip_off[atom0]};
+  for (int base = warp * A; base < Na; base += NW * A) {
+    const int il = base + aslot;
+    if (il < Na) {
+      float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      const float pe = tersoff_atom<ZC, NT, FORCE>(geo, C, il, fsm, G, g, v);
+      if (!FORCE) {
+        red[threadIdx.x] += (double)pe;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) red[(k + 1) * BLK + threadIdx.x] += (double)v[k];
+      }
+    }
+  }
+  if (!FORCE) {
+    red[7 * BLK + threadIdx.x] = 0.0;
+    fold_item(it, P, S.Nc, red, res);
+    return;
+  }
+  __syncthreads();
+  double ferr = 0.0;
+  const int N = S.N, Nf = S.N_force;
+  for (int base = warp * A; base < Na; base += NW * A) {
     const int il = base + aslot;
     if (il < Na) {
       const int i = atom0 + il;
-      float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      const float pe = tersoff_atom<ZC, FORCE>(S, C, i, S.NN[i], fsm, bond0, G, g, v);
-      if (!FORCE) {
-        acc[0] += (double)pe;
+      const int b0 = geo.boff[il] - bond0, Z = geo.nn[il];
+      float Fx = 0.f, Fy = 0.f, Fz = 0.f;
+      for (int j = 0; j < Z; ++j) {
+        const int bl = b0 + j, rl = geo.rev[b0 + j] - bond0;
+        Fx += fsm[(bl * 3 + 0) * G + g] - fsm[(rl * 3 + 0) * G + g];
+        Fy += fsm[(bl * 3 + 1) * G + g] - fsm[(rl * 3 + 1) * G + g];
+        Fz += fsm[(bl * 3 + 2) * G + g] - fsm[(rl * 3 + 2) * G + g];
+      }
+      const double dx = (double)Fx - (double)S.force_ref[i];
+      const double dy = (double)Fy - (double)S.force_ref[i + N];
+      const double dz = (double)Fz - (double)S.force_ref[i + 2 * (size_t)N];
+      ferr += dx * dx + dy * dy + dz * dz;
+      if (fdump && p < P) {
+        fdump[((size_t)p * 3 + 0) * Nf + i] = Fx;
+        fdump[((size_t)p * 3 + 1) * Nf + i] = Fy;
+        fdump[((size_t)p * 3 + 2) * Nf + i] = Fz;
+      }
+    }
+  }
+  __syncthreads();  // the fold overwrites the f_ij scratch
 #pragma unroll
-        for (int k = 0; k < 6; ++k) acc[1 + k] += (double)v[k];
-      }
-    }
-  }
-  if (FORCE) {
-    __syncthreads();
-    const int N = S.N, Nf = S.N_force;
-    for (int base = warp * A; base < Na; base += kWarps * A) {
-      const int il = base + aslot;
-      if (il < Na) {
-        const int i = atom0 + il;
-        const int b0 = S.off[i], Z = S.NN[i];
-        float Fx = 0.f, Fy = 0.f, Fz = 0.f;
-        for (int j = 0; j < Z; ++j) {
-          const int bl = b0 + j - bond0, rl = S.rev[b0 + j] - bond0;
-          Fx += fsm[(bl * 3 + 0) * G + g] - fsm[(rl * 3 + 0) * G + g];
-          Fy += fsm[(bl * 3 + 1) * G + g] - fsm[(rl * 3 + 1) * G + g];
-          Fz += fsm[(bl * 3 + 2) * G + g] - fsm[(rl * 3 + 2) * G + g];
-        }
-        const double dx = (double)Fx - (double)S.force_ref[i];
-        const double dy = (double)Fy - (double)S.force_ref[i + N];
-        const double dz = (double)Fz - (double)S.force_ref[i + 2 * (size_t)N];
-        acc[7] += dx * dx + dy * dy + dz * dz;
-        if (fdump && p < P) {
-          fdump[((size_t)p * 3 + 0) * Nf + i] = Fx;
-          fdump[((size_t)p * 3 + 1) * Nf + i] = Fy;
-          fdump[((size_t)p * 3 + 2) * Nf + i] = Fz;
-        }
-      }
-    }
-  }
-  reduce_item(it, P, S.Nc, acc, smem, res);
+  for (int k = 0; k < 7; ++k) red[k * BLK + threadIdx.x] = 0.0;
+  red[7 * BLK + threadIdx.x] = ferr;
+  fold_item(it, P, S.Nc, red, res);
 }
 
 // --------------------------------------------------------------------------- RI / NN2B
 // RI pair term (ri.cu:77-110) with the geometry-only Coulomb pieces precomputed:
 // gri = (1/d, 1/d^6, erfc(alpha d)/d, erfc(alpha d)/d^2 + 2 alpha/sqrt(pi) exp(-alpha^2 d^2)/d).
 // Returns U(d) in p2 and dU/dd in fd.
-__device__ __forceinline__ void ri_pair(const Consts& k, int t, float d, float4 w, float& p2, float& fd) {
-  const float a = k[RC_A + t], b = k[RC_B + t], c = k[RC_C + t], qq = k[RC_QQ + t];
-  const float rc = k[RC_RC], vrc = k[RC_VRC], dvrc = k[RC_DVRC];
+struct RIC {  // the lane's RI constants, loaded once per work item
+  float qq[3], a[3], b[3], c6[3], c[3], rc, vrc, dvrc, lr, la, cr, ca, r0;
+};
+
+__device__ __forceinline__ void load_ri(const Consts& k, RIC& R) {
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    R.qq[t] = k[RC_QQ + t];
+    R.a[t] = k[RC_A + t];
+    R.b[t] = k[RC_B + t];
+    R.c[t] = k[RC_C + t];
+    R.c6[t] = 6.0f * R.c[t];
+  }
+  R.rc = k[RC_RC];
+  R.vrc = k[RC_VRC];
+  R.dvrc = k[RC_DVRC];
+  R.lr = k[RC_LR];
+  R.la = k[RC_LA];
+  R.cr = k[RC_CR];
+  R.ca = k[RC_CA];
+  R.r0 = k[RC_R0];
+}
+
+__device__ __forceinline__ void ri_pair(const RIC& R, int t, float d, float4 w, float& p2, float& fd) {
+  const float a = t == 0 ? R.a[0] : (t == 1 ? R.a[1] : R.a[2]);
+  const float b = t == 0 ? R.b[0] : (t == 1 ? R.b[1] : R.b[2]);
+  const float c = t == 0 ? R.c[0] : (t == 1 ? R.c[1] : R.c[2]);
+  const float c6 = t == 0 ? R.c6[0] : (t == 1 ? R.c6[1] : R.c6[2]);
+  const float qq = t == 0 ? R.qq[0] : (t == 1 ? R.qq[1] : R.qq[2]);
   const float ex = expf(-d * b);
-  p2 = a * ex - c * w.y + qq * (w.z - vrc - dvrc * (d - rc));
-  fd = 6.0f * c * w.y * w.x - a * ex * b - qq * (w.w + dvrc);
+  p2 = a * ex - c * w.y + qq * (w.z - R.vrc - R.dvrc * (d - R.rc));
+  fd = c6 * w.y * w.x - a * ex * b - qq * (w.w + R.dvrc);
   if (t == 1) {
-    const float lr = k[RC_LR], la = k[RC_LA], dr = d - k[RC_R0];
-    const float fr = k[RC_CR] * expf(-lr * dr);
-    const float fa = k[RC_CA] * expf(-la * dr);
+    const float dr = d - R.r0;
+    const float fr = R.cr * expf(-R.lr * dr);
+    const float fa = R.ca * expf(-R.la * dr);
     p2 += fr - fa;
-    fd += -lr * fr + la * fa;
+    fd += -R.lr * fr + R.la * fa;
   }
 }
 
@@ -435,6 +543,8 @@ __global__ void __launch_bounds__(kBlock) pair_batched(const JobView* __restrict
   const int p = it.p0 + lane;
   const int pl = p < P ? p : it.p0;
   const Consts kc{J.consts, Pstride, pl};
+  RIC R;
+  if (KIND == 1) load_ri(kc, R);
   float* wsm = reinterpret_cast<float*>(smem + (size_t)kWarps * 32 * kResK * sizeof(double));
   if (KIND == 2) {
     for (int t = threadIdx.x; t < nv * 32; t += blockDim.x) {
@@ -455,12 +565,13 @@ __global__ void __launch_bounds__(kBlock) pair_batched(const JobView* __restrict
     const int bbeg = FORCE ? S.off[i] : S.half_off[i];
     const int bend = S.off[i + 1];
     double Fx = 0, Fy = 0, Fz = 0;
+#pragma unroll 2
     for (int b = bbeg; b < bend; ++b) {
       const float4 q = __ldg(&S.g32[b]);
       const float d = q.w;
       float p2, fd;
       if (KIND == 1) {
-        ri_pair(kc, S.ptype[b], d, __ldg(&S.gri[b]), p2, fd);
+        ri_pair(R, S.ptype[b], d, __ldg(&S.gri[b]), p2, fd);
       } else {
         float f2raw;
         nn_pair<NMAX>(wl, nn, d, p2, f2raw);
@@ -560,6 +671,12 @@ __global__ void fitness_jobs(const JobView* __restrict__ jobs, const int2* __res
 namespace {
 constexpr size_t kRedBytes = (size_t)kWarps * 32 * kResK * sizeof(double);
 constexpr size_t kForceSmemTarget = 96 * 1024;  // two CTAs per SM
+constexpr size_t kStageTarget = 110 * 1024;     // force scratch + staged geometry, two CTAs per SM
+// Energy/virial Tersoff items run in 128-thread CTAs (more resident warps per SM at ~115
+// registers per thread) and read their geometry through L1: staging it in shared memory
+// would cap the CTAs per SM without making the per-atom loads cheaper (measured).
+constexpr int kBlockEV = 128;
+constexpr bool kStageEV = false;
 constexpr size_t kSmemMax = 220 * 1024;
 
 int zclass_of(int z) { return z <= 4 ? 4 : (z <= 8 ? 8 : (z <= 16 ? 16 : 0)); }
@@ -597,6 +714,7 @@ JobView make_job_view(const Engine* e, const Plan* plan) {
   j.P = plan->P;
   j.Pstride = plan->Pstride;
   j.Nc_force = d.Nc_force;
+  j.ri_fixed_rc = d.ri_fixed_rc;
   j.tp = NNTaper{e->spec.nn_r1, e->spec.nn_r2, (float)(M_PI / ((double)e->spec.nn_r2 - e->spec.nn_r1)),
                  e->spec.nn_consistent};
   j.pop = plan->d_pop;
@@ -662,7 +780,8 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
   const TrainingSet& ts = e->ts;
   const bool tersoff = d.potential_type == 1 || d.potential_type == 2;
   const int kind = tersoff ? 0 : (d.potential_type == 0 ? 1 : 2);
-  const int nmax = kind == 2 ? nmax_of(d.num_neurons) : 0;
+  // NN2B: register-array size of the MLP; Tersoff: number of atom types (kernel template)
+  const int nmax = kind == 2 ? nmax_of(d.num_neurons) : (kind == 0 ? d.num_types : 0);
   if (kind == 2 && nmax == 0) {
     set_error("batched NN2B supports up to 32 neurons per layer (got %d).", d.num_neurons);
     return GPUGA_ERR_UNSUPPORTED;
@@ -691,6 +810,8 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
     const long long Bc = (long long)e->h_off[ts.Na_sum[c] + Na] - e->h_off[ts.Na_sum[c]];
     int zc = 0, G = 32;
     size_t smem = kRedBytes;
+    bool staged = false;
+    size_t fbytes = 0;
     if (kind == 0) {
       zc = zclass_of(e->h_zmax[c]);
       if (zc == 0) {
@@ -698,6 +819,10 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
                   e->h_zmax[c]);
         return GPUGA_ERR_UNSUPPORTED;
       }
+      long long Tc = 0;
+      for (int k = 0; k < Na; ++k) Tc += (long long)e->h_NN[ts.Na_sum[c] + k] * e->h_NN[ts.Na_sum[c] + k];
+      const size_t stage = ((size_t)Bc * 16 + (size_t)Tc * 4 + (size_t)Na * 12 + (force ? (size_t)Bc * 4 : 0) +
+                            (size_t)Bc + 15) & ~(size_t)15;
       if (force) {
         const size_t per_ind = (size_t)Bc * 3 * sizeof(float);
         while (G > 1 && per_ind * G > kForceSmemTarget) G >>= 1;
@@ -705,7 +830,22 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
           set_error("configuration %d needs %zu bytes of force scratch per individual.", c, per_ind);
           return GPUGA_ERR_UNSUPPORTED;
         }
-        smem = std::max(smem, per_ind * G);
+        // stage the geometry too when it fits beside the scratch of >= 4 individuals
+        int Gs = G;
+        while (Gs > 4 && ((per_ind * Gs + 15) & ~(size_t)15) + stage > kStageTarget) Gs >>= 1;
+        if (((per_ind * Gs + 15) & ~(size_t)15) + stage <= kStageTarget) {
+          G = Gs;
+          staged = true;
+        }
+        fbytes = (per_ind * G + 15) & ~(size_t)15;
+        smem = std::max(smem, fbytes + (staged ? stage : 0));
+      } else {
+        // energy/virial items: per-lane FP64 sums of the 128-thread CTA, then (optionally) the geometry
+        smem = (size_t)kBlockEV * kResK * sizeof(double);
+        if (kStageEV && stage <= kStageTarget) {
+          staged = true;
+          smem += stage;
+        }
       }
     } else if (kind == 2) {
       smem += (size_t)d.num_vars * 32 * sizeof(float);
@@ -721,7 +861,7 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
     }
     for (int p0 = 0; p0 < P; p0 += G) {
       const int cnt = std::min(G, P - p0);
-      groups[key].push_back({WorkItem{c, p0, G, job}, cf * cnt, (double)Na * cnt, cf * cnt, cs * cnt});
+      groups[key].push_back({WorkItem{c, p0, pack_G(G, staged, fbytes), job}, cf * cnt, (double)Na * cnt, cf * cnt, cs * cnt});
     }
   }
   return GPUGA_OK;
@@ -738,13 +878,18 @@ int set_smem(K kernel) {
 int launch_one(const LaunchSet* ls, const Launch& L, cudaStream_t st, bool configure_only) {
   const dim3 grid(L.count), block(kBlock);
   const WorkItem* items = ls->d_items + L.first;
+#define GPUGA_TERSOFF1(ZC, NT, F)                                                       \
+  do {                                                                                  \
+    constexpr int BLK = F ? kBlock : kBlockEV;                                          \
+    if (configure_only) {                                                               \
+      GPUGA_TRY(set_smem(tersoff_batched<ZC, NT, F, BLK>));                             \
+      break;                                                                            \
+    }                                                                                   \
+    tersoff_batched<ZC, NT, F, BLK><<<grid, dim3(BLK), L.smem, st>>>(ls->d_jobs, items); \
+  } while (0)
 #define GPUGA_TERSOFF(ZC, F)                                                          \
   do {                                                                                \
-    if (configure_only) {                                                             \
-      GPUGA_TRY(set_smem(tersoff_batched<ZC, F>));                                    \
-      break;                                                                          \
-    }                                                                                 \
-    tersoff_batched<ZC, F><<<grid, block, L.smem, st>>>(ls->d_jobs, items);           \
+    if (L.nmax == 2) GPUGA_TERSOFF1(ZC, 2, F); else GPUGA_TERSOFF1(ZC, 1, F);         \
   } while (0)
 #define GPUGA_PAIR(KD, NM, F)                                                         \
   do {                                                                                \
@@ -772,6 +917,7 @@ int launch_one(const LaunchSet* ls, const Launch& L, cudaStream_t st, bool confi
     if (L.force) GPUGA_PAIR(2, 32, true); else GPUGA_PAIR(2, 32, false);
   }
 #undef GPUGA_TERSOFF
+#undef GPUGA_TERSOFF1
 #undef GPUGA_PAIR
   GPUGA_CUDA(cudaGetLastError());
   return GPUGA_OK;

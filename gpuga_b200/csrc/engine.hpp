@@ -53,6 +53,9 @@ struct DevSet {
   double* W_ref = nullptr;
   double norm_force = 0, norm_energy = 0, norm_virial = 0;
   float w_force = 0, w_energy = 0, w_stress = 0;
+  // RI: the Coulomb shift cutoff (parameter 10) is the same for every individual, so the
+  // shifted, damped Coulomb term is precomputed per bond in FP64 (gri.z, gri.w)
+  int ri_fixed_rc = 0;
 };
 
 // One CTA of a batched launch: configuration `config` of job `job` for
@@ -90,7 +93,7 @@ struct NNTaper {
 // buffers of its evaluation.  Several jobs share the same launches.
 struct JobView {
   DevView v;
-  int potential_type, num_types, num_neurons, num_vars, P, Pstride, Nc_force;
+  int potential_type, num_types, num_neurons, num_vars, P, Pstride, Nc_force, ri_fixed_rc;
   NNTaper tp;
   const float* pop;      // [P][num_vars] in [0,1]
   const float* pmin;
@@ -110,7 +113,7 @@ struct JobView {
 struct Launch {
   int kind = 0;        // 0 Tersoff, 1 RI, 2 NN2B
   int zclass = 4;      // Tersoff register-array size
-  int nmax = 0;        // NN2B register-array size
+  int nmax = 0;        // NN2B register-array size; Tersoff: number of atom types
   bool force = false;  // force items (gather pass) vs energy/virial items
   size_t smem = 0;
   int count = 0;

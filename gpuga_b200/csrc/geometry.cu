@@ -126,7 +126,7 @@ constexpr double kRiPiFactor = 0.225675833419103;  // ri.cu:28, 2*alpha/sqrt(pi)
 __global__ void bond_geometry(int N, const int* __restrict__ atom_cfg, const float* __restrict__ box,
                               const float* __restrict__ r, const int* __restrict__ type, const int* __restrict__ off,
                               const int* __restrict__ nbr, const float* __restrict__ img, int potential_type,
-                              int num_types, double4* __restrict__ g64, float4* __restrict__ g32,
+                              int num_types, double rc_fixed, double4* __restrict__ g64, float4* __restrict__ g32,
                               float4* __restrict__ gri, int* __restrict__ rev, int* __restrict__ half_off,
                               uint8_t* __restrict__ ptype) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -149,7 +149,16 @@ __global__ void bond_geometry(int N, const int* __restrict__ atom_cfg, const flo
       const double dinv3 = dinv * dinv * dinv;
       const double e1 = erfc(kRiAlpha * d) * dinv;
       const double e2 = e1 * dinv + kRiPiFactor * dinv * exp(-kRiAlpha * kRiAlpha * d * d);
-      gri[b] = make_float4((float)dinv, (float)(dinv3 * dinv3), (float)e1, (float)e2);
+      if (rc_fixed > 0) {
+        // whole shifted-force Coulomb term (ri.cu:92-94) for the common cutoff, in FP64
+        const double v_rc = erfc(kRiAlpha * rc_fixed) / rc_fixed;
+        const double dv_rc = -erfc(kRiAlpha * rc_fixed) / (rc_fixed * rc_fixed) -
+                             kRiPiFactor * exp(-kRiAlpha * kRiAlpha * rc_fixed * rc_fixed) / rc_fixed;
+        gri[b] = make_float4((float)dinv, (float)(dinv3 * dinv3), (float)(e1 - v_rc - dv_rc * (d - rc_fixed)),
+                             (float)(e2 + dv_rc));
+      } else {
+        gri[b] = make_float4((float)dinv, (float)(dinv3 * dinv3), (float)e1, (float)e2);
+      }
     }
     int rb = off[j];  // minimal_tersoff.cu:368: slot 0 when the reverse is absent
     for (int k = off[j]; k < off[j + 1]; ++k)
@@ -291,8 +300,14 @@ int build_geometry(Engine* e) {
   GPUGA_TRY(e->alloc(&d.half_off, N));
   GPUGA_TRY(e->alloc(&d.ptype, std::max(B, 1)));
   if (d.potential_type == 0) GPUGA_TRY(e->alloc(&d.gri, std::max(B, 1)));
+  double rc_fixed = 0.0;
+  if (d.potential_type == 0 && e->spec.pmin.size() > 10 && e->spec.pmin[10] == e->spec.pmax[10] &&
+      e->spec.pmin[10] > 0) {
+    rc_fixed = e->spec.pmin[10];
+    d.ri_fixed_rc = 1;
+  }
   bond_geometry<<<(N + 127) / 128, 128, 0, st>>>(N, d_atom_cfg, d.h, d.r, d.type, d.off, d.nbr, img,
-                                                 d.potential_type, d.num_types, d.g64, d.g32, d.gri, d.rev,
+                                                 d.potential_type, d.num_types, rc_fixed, d.g64, d.g32, d.gri, d.rev,
                                                  d.half_off, d.ptype);
   GPUGA_CUDA(cudaGetLastError());
 

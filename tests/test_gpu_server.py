@@ -20,7 +20,7 @@ GENS = 6
 @pytest.fixture(scope="module")
 def job_dirs(built_oracle, tmp_path_factory):
     dirs = []
-    for cfg, Nc, P in [(1, 8, 40), (2, 12, 60), (3, 4, 20), (1, 6, 30)]:
+    for cfg, Nc, P in [(1, 8, 40), (2, 12, 60), (3, 4, 20), (1, 6, 40)]:  # parent_number = P/2, a multiple of 10
         d, data = synthetic_dir(built_oracle, cfg, Nc, str(tmp_path_factory.mktemp(f"job{cfg}_{Nc}")))
         with open(f"{d}/ga.in", "w") as f:
             f.write(f"maximum_generation 50\npopulation_size {P}\nparent_number {P // 2}\nmutation_rate 0.2\n")
