@@ -151,6 +151,23 @@ def measured_peaks() -> dict:
         return {}
 
 
+def ncu_traffic(kernel: str, workload: int, units: float):
+    """DRAM bytes (read + write) of one launch of `kernel`, from the ncu capture summarised in
+    profiles/dram_traffic.md (lines `traffic: workload=W kernel=K units=U bytes=B`), or None
+    when that launch shape was not captured."""
+    try:
+        lines = open(os.path.join(ROOT, "profiles", "dram_traffic.md")).read().splitlines()
+    except OSError:
+        return None
+    for line in lines:
+        if not line.startswith("traffic:"):
+            continue
+        kv = dict(tok.split("=", 1) for tok in line.split()[1:])
+        if int(kv["workload"]) == workload and kv["kernel"] == kernel and float(kv["units"]) == units:
+            return float(kv["bytes"])
+    return None
+
+
 # ----------------------------------------------------------------------------- workload
 def oracle_evaluator():
     from oracle import oracle
@@ -241,7 +258,8 @@ def run_ours(args, dist: Dist):
     value = dist.world * P * Natoms * nsteps / (total_ms / 1e3)
     fit_dev = fit.cpu().numpy().copy()
 
-    # ---- per-launch device times (separate pass, launches bracketed by events on their own streams)
+    # ---- per-launch device times (separate pass of K steps; the launches of a step run one after
+    # another on this stream while timing is on, each bracketed by its own events)
     _lib.check(L.gpuga_kernel_timing(h, P, 1))
     for k in range(nsteps):
         flush.zero_()
@@ -259,11 +277,16 @@ def run_ours(args, dist: Dist):
                          "ctas": int(r[3]), "units": r[4], "flops": r[5], "sfu_calls": r[6], "ms": r[7],
                          "tflops": (r[5] / (r[7] * 1e-3) / 1e12) if r[7] > 0 else None})
     dom = max(launches, key=lambda x: x["ms"])
+    gen_flops = sum(x["flops"] for x in launches)
+    traffic = ncu_traffic(dom["kernel"], args.workload, dom["units"])
     roofline = {"bound": "fp32", "kernel": dom["kernel"], "achieved": dom["tflops"], "peak": peak_fp32.value,
                 "unit": "TFLOP/s", "frac": dom["tflops"] / peak_fp32.value if dom["tflops"] else None,
-                "traffic": None, "peak_source": "measured: FFMA-chain calibration kernel on this GPU",
+                "traffic": traffic, "peak_source": "measured: FFMA-chain calibration kernel on this GPU",
                 "algorithmic": "FP32 flops of the batched formulation (FMA=2), transcendentals separate",
-                "ms_per_launch": dom["ms"], "launches": launches}
+                "ms_per_launch": dom["ms"], "launches": launches,
+                "generation": {"flops": gen_flops, "ms": ms_per_step,
+                               "achieved": gen_flops / (ms_per_step * 1e-3) / 1e12,
+                               "frac": gen_flops / (ms_per_step * 1e-3) / 1e12 / peak_fp32.value}}
 
     # ---- e2e through the public C ABI with host buffers
     e2e_ms = []

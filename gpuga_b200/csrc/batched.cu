@@ -193,6 +193,41 @@ __device__ __forceinline__ void reduce_item(const WorkItem& it, int P, int Nc, d
   fold_item(it, P, Nc, red, res);
 }
 
+// Geometry of one configuration as a CTA sees it: in shared memory when the
+// work item was staged, otherwise the global arrays offset to the
+// configuration's first atom / bond.  Bond indices are local.
+struct Geo {
+  const float4* g;     // [Bc] (unit vector, d)
+  const uint8_t* pt;   // [Bc] pair set
+  const int* rev;      // [Bc] reverse bond (global numbering; subtract bond0)
+  const int* nn;       // [Na]
+  const int* boff;     // [Na] bond offset (global numbering; subtract bond0)
+  int bond0;
+};
+
+// Copies configuration c's geometry into shared memory with all threads of
+// the CTA (independent vector loads, then one barrier).
+__device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int Na, bool force, unsigned char* base) {
+  const int bond0 = S.off[atom0], bond1 = S.off[atom0 + Na];
+  const int Bc = bond1 - bond0;
+  float4* sg = reinterpret_cast<float4*>(base);
+  int* snn = reinterpret_cast<int*>(sg + Bc);
+  int* sbo = snn + Na;
+  int* srev = sbo + Na;
+  uint8_t* spt = reinterpret_cast<uint8_t*>(srev + (force ? Bc : 0));
+  for (int k = threadIdx.x; k < Bc; k += blockDim.x) {
+    sg[k] = __ldg(&S.g32[bond0 + k]);
+    spt[k] = S.ptype[bond0 + k];
+    if (force) srev[k] = S.rev[bond0 + k];
+  }
+  for (int k = threadIdx.x; k < Na; k += blockDim.x) {
+    snn[k] = S.NN[atom0 + k];
+    sbo[k] = S.off[atom0 + k];
+  }
+  __syncthreads();
+  return Geo{sg, spt, srev, snn, sbo, bond0};
+}
+
 // One atom of the minimal Tersoff potential (minimal_tersoff.cu:122-405) for
 // the lane's parameter vector.  Returns the site energy; writes the partial
 // forces f_ij (FORCE) or adds -r_ij (x) f_ij into v[6] (energy/virial items).
@@ -202,52 +237,6 @@ __device__ __forceinline__ void reduce_item(const WorkItem& it, int P, int Nc, d
 // the reference's f_ij (minimal_tersoff.cu:250-307) is
 //   f_ij = 1/2 [ (A'_j - fc'_j sum_k T_k g_jk - m_j sum_k q_jk cos_jk) u_j + m_j sum_k q_jk u_k ]
 // with q_jk = beta (cos_jk - h) (S_j fc_k + T_k) and m_j = -2 fc_j / d_j.
-// Geometry of one configuration as a CTA sees it: in shared memory when the
-// work item was staged, otherwise the global arrays offset to the
-// configuration's first atom / bond / triplet.  All indices are local.
-struct Geo {
-  const float4* g;     // [Bc] (unit vector, d)
-  const uint8_t* pt;   // [Bc] pair set
-  const float* cs;     // [Tc] cos(theta) blocks
-  const int* rev;      // [Bc] reverse bond (global numbering; subtract bond0)
-  const int* nn;       // [Na]
-  const int* boff;     // [Na] bond offset (global numbering; subtract bond0)
-  const int* toff;     // [Na] triplet offset (global numbering; subtract trip0)
-  int bond0, trip0;
-};
-
-// Copies configuration c's geometry into shared memory with all threads of
-// the CTA (independent vector loads, then one barrier).
-__device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int Na, bool force, unsigned char* base) {
-  const int bond0 = S.off[atom0], bond1 = S.off[atom0 + Na];
-  const int trip0 = S.trip_off[atom0], trip1 = S.trip_off[atom0 + Na];
-  const int Bc = bond1 - bond0, Tc = trip1 - trip0;
-  float4* sg = reinterpret_cast<float4*>(base);
-  float* scs = reinterpret_cast<float*>(sg + Bc);
-  int* snn = reinterpret_cast<int*>(scs + Tc);
-  int* sbo = snn + Na;
-  int* sto = sbo + Na;
-  int* srev = sto + Na;
-  uint8_t* spt = reinterpret_cast<uint8_t*>(srev + (force ? Bc : 0));
-  for (int k = threadIdx.x; k < Bc; k += blockDim.x) {
-    sg[k] = __ldg(&S.g32[bond0 + k]);
-    spt[k] = S.ptype[bond0 + k];
-    if (force) srev[k] = S.rev[bond0 + k];
-  }
-  for (int k = threadIdx.x; k < Tc; k += blockDim.x) scs[k] = __ldg(&S.cosm[trip0 + k]);
-  for (int k = threadIdx.x; k < Na; k += blockDim.x) {
-    snn[k] = S.NN[atom0 + k];
-    sbo[k] = S.off[atom0 + k];
-    sto[k] = S.trip_off[atom0 + k];
-  }
-  __syncthreads();
-  return Geo{sg, spt, scs, srev, snn, sbo, sto, bond0, trip0};
-}
-
-__device__ __forceinline__ size_t staged_bytes(int Na, int Bc, int Tc, bool force) {
-  return (size_t)Bc * 16 + (size_t)Tc * 4 + (size_t)Na * 12 + (force ? (size_t)Bc * 4 : 0) + (size_t)Bc;
-}
-
 template <int ZC, int NT, bool FORCE>
 __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C, int il, float* fsm, int G, int g,
                                               float (&v)[6]) {
@@ -284,7 +273,8 @@ __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C,
     }
   }
   // pass B: bond order, site energy and the per-bond force scalars
-  const float* cs = geo.cs + (geo.toff[il] - geo.trip0);
+  // cos(theta_jik) = u_j . u_k from the FP32 unit vectors (as accurate as a stored FP32 cosine)
+  auto cosine = [&](int j, int k) { return fmaf(uz[j], uz[k], fmaf(uy[j], uy[k], ux[j] * ux[k])); };
   float Ap[ZC], Sb[ZC], Tb[ZC];
   float pe = 0.f;
 #pragma unroll
@@ -295,7 +285,7 @@ __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C,
 #pragma unroll
       for (int k = 0; k < ZC; ++k) {
         if (k < Z && k != j) {
-          const float x = cs[j * Z + k] - C.h;
+          const float x = cosine(j, k) - C.h;
           zeta = fmaf(fc[k] * C.beta, x * x, zeta);
         }
       }
@@ -304,7 +294,7 @@ __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C,
         const float zn = powf(zeta, C.en);
         const float opz = 1.0f + zn;
         b = powf(opz, C.mhon);
-        bp = -0.5f * b * zn * __frcp_rn(opz * zeta);
+        bp = __fdividef(-0.5f * b * zn, opz * zeta);
       }
       const int s = NT == 2 ? st[j] : 0;
       const float e = fr[j] - b * fa[j];
@@ -325,7 +315,7 @@ __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C,
 #pragma unroll
       for (int k = 0; k < ZC; ++k) {
         if (k < Z && k != j) {
-          const float cjk = cs[j * Z + k];
+          const float cjk = cosine(j, k);
           const float bx = C.beta * (cjk - C.h);
           const float g = bx * (cjk - C.h);
           const float q = bx * fmaf(Sj, fc[k], Tb[k]);
@@ -336,7 +326,7 @@ __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C,
           Vz = fmaf(q, uz[k], Vz);
         }
       }
-      const float m = -2.0f * fc[j] * __frcp_rn(dd[j]);
+      const float m = __fdividef(-2.0f * fc[j], dd[j]);
       const float cu = 0.5f * (Ap[j] - fcp[j] * sumG - m * accC);
       const float cv = 0.5f * m;
       const float fx = fmaf(cu, ux[j], cv * Vx);
@@ -394,8 +384,7 @@ __global__ void __launch_bounds__(BLK) tersoff_batched(const JobView* __restrict
   }
   const Geo geo = item_staged(it)
                       ? stage_geometry(S, atom0, Na, FORCE, smem + front)
-                      : Geo{S.g32 + bond0, S.ptype + bond0, S.cosm + S.trip_off[atom0], S.rev + bond0,
-                            S.NN + atom0, S.off + atom0, S.trip_off + atom0, bond0, S.trip_off[atom0]};
+                      : Geo{S.g32 + bond0, S.ptype + bond0, S.rev + bond0, S.NN + atom0, S.off + atom0, bond0};
   for (int base = warp * A; base < Na; base += NW * A) {
     const int il = base + aslot;
     if (il < Na) {
@@ -491,40 +480,81 @@ __device__ __forceinline__ void ri_pair(const RIC& R, int t, float d, float4 w, 
   }
 }
 
-// NN2B value and derivative (nn2b.cu:49-78) with the lane's weights in shared memory,
-// laid out [parameter][32 lanes].
+// NN2B value and derivative (nn2b.cu:49-78) for the lane's weights, held in
+// shared memory as float4 groups so that each 16-byte load feeds eight FMAs:
+//   W1[a][m/4][lane] (hidden-to-hidden, row a), V[v][a/4][lane] for v = w0, b0, b1, w2,
+//   b2[lane]; NMAX pads n to a multiple of 4 with zero weights.
 template <int NMAX>
-__device__ __forceinline__ void nn_pair(const float* __restrict__ wl, int n, float d, float& p2, float& f2) {
+struct NNSmem {
+  static constexpr int Q = NMAX / 4;
+  static constexpr size_t floats = (size_t)32 * (NMAX * NMAX + 4 * NMAX + 1);
+  // float offset of parameter m (nn2b.cu:33-46 order) of lane l
+  __device__ static size_t offset(int m, int n, int l) {
+    auto vec = [&](int v, int a) { return ((size_t)((v * Q + a / 4) * 32 + l)) * 4 + a % 4; };
+    const size_t w1_floats = (size_t)NMAX * Q * 32 * 4;
+    if (m < n) return w1_floats + vec(0, m);
+    if (m < 2 * n) return w1_floats + vec(1, m - n);
+    if (m < 2 * n + n * n) {
+      const int idx = m - 2 * n, a = idx / n, mm = idx % n;
+      return ((size_t)((a * Q + mm / 4) * 32 + l)) * 4 + mm % 4;
+    }
+    if (m < n * (n + 3)) return w1_floats + vec(2, m - n * (n + 2));
+    if (m < n * (n + 4)) return w1_floats + vec(3, m - n * (n + 3));
+    return w1_floats + (size_t)4 * Q * 32 * 4 + l;
+  }
+};
+
+template <int NMAX>
+__device__ __forceinline__ void nn_pair(const float* __restrict__ wsm, int lane, int n, float d, float& p2,
+                                        float& f2) {
+  constexpr int Q = NMAX / 4;
+  const float4* W1 = reinterpret_cast<const float4*>(wsm);
+  const float4* V = W1 + NMAX * Q * 32;
+  const float b2 = wsm[(size_t)(NMAX * Q * 32 + 4 * Q * 32) * 4 + lane];
   float x1[NMAX], y1[NMAX];
 #pragma unroll
-  for (int a = 0; a < NMAX; ++a) {
-    x1[a] = y1[a] = 0.f;
-    if (a < n) {
-      const float w0 = wl[a * 32];
-      x1[a] = tanhf(w0 * d - wl[(a + n) * 32]);
-      y1[a] = (1.0f - x1[a] * x1[a]) * w0;
+  for (int q = 0; q < Q; ++q) {
+    const float4 w0 = V[(0 * Q + q) * 32 + lane];
+    const float4 b0 = V[(1 * Q + q) * 32 + lane];
+    const float w0c[4] = {w0.x, w0.y, w0.z, w0.w}, b0c[4] = {b0.x, b0.y, b0.z, b0.w};
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      x1[4 * q + c] = tanhf(w0c[c] * d - b0c[c]);
+      y1[4 * q + c] = (1.0f - x1[4 * q + c] * x1[4 * q + c]) * w0c[c];
     }
   }
   p2 = 0.f;
   f2 = 0.f;
-  for (int a = 0; a < n; ++a) {
-    const float* w1 = wl + (2 * n + a * n) * 32;
-    float x2 = 0.f, y2 = 0.f;
+  const int qa_end = (n + 3) >> 2;
+  for (int qa = 0; qa < qa_end; ++qa) {
+    const float4 b1 = V[(2 * Q + qa) * 32 + lane];
+    const float4 w2 = V[(3 * Q + qa) * 32 + lane];
+    const float b1c[4] = {b1.x, b1.y, b1.z, b1.w}, w2c[4] = {w2.x, w2.y, w2.z, w2.w};
 #pragma unroll
-    for (int m = 0; m < NMAX; ++m) {
-      if (m < n) {
-        const float w = w1[m * 32];
-        x2 = fmaf(w, x1[m], x2);
-        y2 = fmaf(w, y1[m], y2);
+    for (int c = 0; c < 4; ++c) {
+      const int a = 4 * qa + c;
+      if (a < n) {
+        float x2 = 0.f, y2 = 0.f;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+          const float4 w = W1[(a * Q + q) * 32 + lane];
+          x2 = fmaf(w.x, x1[4 * q], x2);
+          y2 = fmaf(w.x, y1[4 * q], y2);
+          x2 = fmaf(w.y, x1[4 * q + 1], x2);
+          y2 = fmaf(w.y, y1[4 * q + 1], y2);
+          x2 = fmaf(w.z, x1[4 * q + 2], x2);
+          y2 = fmaf(w.z, y1[4 * q + 2], y2);
+          x2 = fmaf(w.w, x1[4 * q + 3], x2);
+          y2 = fmaf(w.w, y1[4 * q + 3], y2);
+        }
+        x2 = tanhf(x2 - b1c[c]);
+        y2 *= 1.0f - x2 * x2;
+        p2 = fmaf(w2c[c], x2, p2);
+        f2 = fmaf(w2c[c], y2, f2);
       }
     }
-    x2 = tanhf(x2 - wl[(n * (n + 2) + a) * 32]);
-    y2 *= 1.0f - x2 * x2;
-    const float w2 = wl[(n * (n + 3) + a) * 32];
-    p2 = fmaf(w2, x2, p2);
-    f2 = fmaf(w2, y2, f2);
   }
-  p2 -= wl[(n * (n + 4)) * 32];
+  p2 -= b2;
 }
 
 template <int KIND, int NMAX, bool FORCE>
@@ -547,14 +577,15 @@ __global__ void __launch_bounds__(kBlock) pair_batched(const JobView* __restrict
   if (KIND == 1) load_ri(kc, R);
   float* wsm = reinterpret_cast<float*>(smem + (size_t)kWarps * 32 * kResK * sizeof(double));
   if (KIND == 2) {
+    for (size_t t = threadIdx.x; t < NNSmem<NMAX>::floats; t += blockDim.x) wsm[t] = 0.f;  // zero padding
+    __syncthreads();
     for (int t = threadIdx.x; t < nv * 32; t += blockDim.x) {
       const int m = t >> 5, l = t & 31;
       const int pp = it.p0 + l < P ? it.p0 + l : it.p0;
-      wsm[t] = weights[(size_t)m * Pstride + pp];
+      wsm[NNSmem<NMAX>::offset(m, nn, l)] = weights[(size_t)m * Pstride + pp];
     }
     __syncthreads();
   }
-  const float* wl = wsm + lane;
   const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
   const int N = S.N;
   double acc[kResK];
@@ -574,7 +605,7 @@ __global__ void __launch_bounds__(kBlock) pair_batched(const JobView* __restrict
         ri_pair(R, S.ptype[b], d, __ldg(&S.gri[b]), p2, fd);
       } else {
         float f2raw;
-        nn_pair<NMAX>(wl, nn, d, p2, f2raw);
+        nn_pair<NMAX>(wsm, lane, nn, d, p2, f2raw);
         float fc, fcp;
         cutoff_fn(tp.r1, tp.r2, tp.pf, d, fc, fcp);
         if (tp.consistent) {
@@ -693,12 +724,10 @@ DevView make_view(const DevSet& d) {
   v.NN = d.NN;
   v.off = d.off;
   v.half_off = d.half_off;
-  v.trip_off = d.trip_off;
   v.rev = d.rev;
   v.ptype = d.ptype;
   v.g32 = d.g32;
   v.gri = d.gri;
-  v.cosm = d.cosm;
   v.force_ref = d.force_ref;
   return v;
 }
@@ -819,10 +848,8 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
                   e->h_zmax[c]);
         return GPUGA_ERR_UNSUPPORTED;
       }
-      long long Tc = 0;
-      for (int k = 0; k < Na; ++k) Tc += (long long)e->h_NN[ts.Na_sum[c] + k] * e->h_NN[ts.Na_sum[c] + k];
-      const size_t stage = ((size_t)Bc * 16 + (size_t)Tc * 4 + (size_t)Na * 12 + (force ? (size_t)Bc * 4 : 0) +
-                            (size_t)Bc + 15) & ~(size_t)15;
+      const size_t stage =
+          ((size_t)Bc * 16 + (size_t)Na * 8 + (force ? (size_t)Bc * 4 : 0) + (size_t)Bc + 15) & ~(size_t)15;
       if (force) {
         const size_t per_ind = (size_t)Bc * 3 * sizeof(float);
         while (G > 1 && per_ind * G > kForceSmemTarget) G >>= 1;
@@ -848,7 +875,7 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
         }
       }
     } else if (kind == 2) {
-      smem += (size_t)d.num_vars * 32 * sizeof(float);
+      smem += (size_t)32 * (nmax * nmax + 4 * nmax + 1) * sizeof(float);  // NNSmem<nmax>::floats
     }
     const LaunchKey key{kind, zc, nmax, force ? 1 : 0};
     smem_need[key] = std::max(smem_need[key], smem);
@@ -1007,14 +1034,15 @@ int launchset_collect_timing(LaunchSet* ls) {
 
 // One generation of every job of the set: decode, the batched launches
 // (energy/virial launches on `st`, force launches on the side stream), then
-// the fitness fold.
+// the fitness fold.  While per-launch timing is on, every launch runs on `st`
+// one after another, so that each event pair brackets that launch alone.
 int launchset_enqueue(LaunchSet* ls, cudaStream_t st) {
   const int total = ls->total_individuals;
   decode_jobs<<<(total + 127) / 128, 128, 0, st>>>(ls->d_jobs, ls->d_indmap, total);
   GPUGA_CUDA(cudaGetLastError());
   bool any_side = false;
   for (const Launch& L : ls->launches)
-    if (L.force) any_side = true;
+    if (L.force && !ls->timing) any_side = true;
   if (any_side) {
     GPUGA_CUDA(cudaEventRecord(ls->fork, st));
     GPUGA_CUDA(cudaStreamWaitEvent(ls->side, ls->fork, 0));
@@ -1022,7 +1050,7 @@ int launchset_enqueue(LaunchSet* ls, cudaStream_t st) {
   GPUGA_TRY(launchset_collect_timing(ls));
   for (size_t k = 0; k < ls->launches.size(); ++k) {
     const Launch& L = ls->launches[k];
-    cudaStream_t s = L.force ? ls->side : st;
+    cudaStream_t s = L.force && any_side ? ls->side : st;
     if (ls->timing) GPUGA_CUDA(cudaEventRecord(ls->tev[2 * k], s));
     GPUGA_TRY(launch_one(ls, L, s, false));
     if (ls->timing) GPUGA_CUDA(cudaEventRecord(ls->tev[2 * k + 1], s));

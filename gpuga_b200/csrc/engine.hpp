@@ -3,11 +3,10 @@
 //
 //   configs  Na[Nc], Na_sum[Nc], cfg_zmax[Nc]
 //   atoms    type[N], r[3N] (SoA, FP32 as parsed), NN[N], off[N+1] (CSR into bonds),
-//            half_off[N] (first bond whose neighbor index is > i), trip_off[N+1]
+//            half_off[N] (first bond whose neighbor index is > i)
 //   bonds    nbr[B], rev[B] (reverse bond), ptype[B] (pair set / RI pair type),
 //            g32[B] float4 (unit vector, d), g64[B] double4 (x,y,z,d),
 //            gri[B] float4 (RI geometry-only terms), image shift from the FP32 MIC
-//   triplets cosm[sum Z_i^2] FP32 cos(theta_ijk), row j col k of atom i's Z_i x Z_i block
 //   targets  force_ref[3N], E_ref[Nc], W_ref[6Nc] (FP64 copies of the FP32 inputs)
 //
 // Bond vectors use the periodic image chosen by the reference's FP32 rule and
@@ -40,14 +39,12 @@ struct DevSet {
   int* NN = nullptr;
   int* off = nullptr;
   int* half_off = nullptr;
-  int* trip_off = nullptr;
   int* nbr = nullptr;
   int* rev = nullptr;
   uint8_t* ptype = nullptr;
   float4* g32 = nullptr;
   double4* g64 = nullptr;
   float4* gri = nullptr;
-  float* cosm = nullptr;
   float* force_ref = nullptr;
   double* E_ref = nullptr;
   double* W_ref = nullptr;
@@ -75,12 +72,10 @@ struct DevView {
   const int* NN;
   const int* off;
   const int* half_off;
-  const int* trip_off;
   const int* rev;
   const uint8_t* ptype;
   const float4* g32;
   const float4* gri;
-  const float* cosm;
   const float* force_ref;
 };
 

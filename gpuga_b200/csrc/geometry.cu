@@ -176,22 +176,6 @@ __global__ void bond_geometry(int N, const int* __restrict__ atom_cfg, const flo
   half_off[i] = hstart;
 }
 
-// Three-body cosines cos(theta_jik) for every ordered pair of atom i's bonds.
-__global__ void triplet_cosines(int N, const int* __restrict__ off, const int* __restrict__ trip_off,
-                                const double4* __restrict__ g64, float* __restrict__ cosm) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  const int b0 = off[i], Z = off[i + 1] - b0;
-  float* out = cosm + trip_off[i];
-  for (int j = 0; j < Z; ++j) {
-    const double4 a = g64[b0 + j];
-    for (int k = 0; k < Z; ++k) {
-      const double4 b = g64[b0 + k];
-      out[j * Z + k] = (float)((a.x * b.x + a.y * b.y + a.z * b.z) / (a.w * b.w));
-    }
-  }
-}
-
 // Bond geometry for lists in the reference layout NL[k*N + i]: the FP32 rule
 // picks the image, the vector is then evaluated in FP64; rev holds the slot of
 // the reverse bond (slot 0 of the neighbor when absent, minimal_tersoff.cu:368).
@@ -311,24 +295,6 @@ int build_geometry(Engine* e) {
                                                  d.half_off, d.ptype);
   GPUGA_CUDA(cudaGetLastError());
 
-  if (d.potential_type == 1 || d.potential_type == 2) {
-    std::vector<int> trip(N + 1, 0);
-    long long t = 0;
-    for (int i = 0; i < N; ++i) {
-      trip[i] = (int)t;
-      t += (long long)e->h_NN[i] * e->h_NN[i];
-    }
-    if (t > (1LL << 31) - 1) {
-      set_error("too many three-body terms (%lld).", t);
-      return GPUGA_ERR_UNSUPPORTED;
-    }
-    trip[N] = (int)t;
-    GPUGA_TRY(e->alloc(&d.trip_off, N + 1));
-    GPUGA_TRY(e->alloc(&d.cosm, std::max<long long>(t, 1)));
-    GPUGA_CUDA(cudaMemcpyAsync(d.trip_off, trip.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice, st));
-    triplet_cosines<<<(N + 127) / 128, 128, 0, st>>>(N, d.off, d.trip_off, d.g64, d.cosm);
-    GPUGA_CUDA(cudaGetLastError());
-  }
   GPUGA_CUDA(cudaStreamSynchronize(st));
   cudaFree(img);
   cudaFree(d_atom_cfg);

@@ -125,9 +125,10 @@ int gpuga_batched_forces(gpuga_engine* e, int P, const float* pop01, float* forc
  * {kind (0 Tersoff, 1 RI, 2 NN2B), register class, force items?, CTAs, (individual, atom) units,
  *  algorithmic FP32 flops, transcendental calls, mean device ms per generation while timing is on}. */
 int gpuga_plan_info(gpuga_engine* e, int P, int* n_launches, double* per_launch, int cap);
-/* Records CUDA events around every batched launch of population size P on the launch's own
- * stream (eager launches only: gpuga_fitness_device, or gpuga_fitness with use_graph = 0);
- * enabling or disabling resets the accumulated times. */
+/* Records CUDA events around every batched launch of population size P (eager launches only:
+ * gpuga_fitness_device, or gpuga_fitness with use_graph = 0).  While timing is on, the launches
+ * of a generation run one after another on the caller's stream, so each duration is that
+ * launch's own; enabling or disabling resets the accumulated times. */
 int gpuga_kernel_timing(gpuga_engine* e, int P, int enable);
 /* Measured FP32 CUDA-core FMA throughput of `device` (TFLOP/s), for roofline fractions. */
 int gpuga_calibrate_fp32(int device, double* tflops);
