@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--serving", action="store_true", help="serving benchmark (workload 5) instead")
     ap.add_argument("--serving-jobs", type=int, default=32)
     ap.add_argument("--serving-generations", type=int, default=20)
+    ap.add_argument("--ga-generations", type=int, default=20,
+                    help="generations of the full GA loop timed on the host and on the device loop (0 = skip)")
     return ap.parse_args()
 
 
@@ -306,6 +308,9 @@ def run_ours(args, dist: Dist):
     p50 = float(np.percentile(e2e_sorted, 50))
     p99 = float(np.percentile(e2e_sorted, 99))
 
+    # ---- whole GA generations (fitness + selection/crossover/mutation): host loop vs device loop
+    ga_loop = measure_ga_loops(e, P, args.ga_generations) if args.ga_generations > 0 else None
+
     # ---- plain FP64 one-individual-per-launch path (denominator of the batched speed-up)
     npl = min(args.plain_individuals, P)
     plain_pop = pops_h[nwarm + nsteps - 1][:npl]
@@ -335,6 +340,7 @@ def run_ours(args, dist: Dist):
         "plain_fp64": {"value": plain_value, "unit": UNIT, "individuals": npl,
                        "speedup_batched_vs_plain_fp64": value / plain_value,
                        "max_rel_fitness_err_vs_fp64": float(rel.max()), "ranking_identical": rank_same},
+        "ga_loop": ga_loop,
         "clocks": clock_info,
         "measured_peaks": {k: measured_peaks().get(k) for k in ("hbm_gbs", "bf16_tflops", "sm_max_mhz")},
         "fitness_checksum": float(np.sum(fit_dev)),
@@ -343,6 +349,31 @@ def run_ours(args, dist: Dist):
         result["cpu_baseline"] = cpu_baseline(data, args.cpu_seconds)
     e.close()
     return result
+
+
+def measure_ga_loops(e, P: int, gens: int) -> dict:
+    """Wall time per GA generation (ga.cu:78-92: fitness, sort, output line, crossover, mutation) with the
+    host loop (gpuga_ga_step) and the device-resident loop (gpuga_ga_advance); both give identical
+    ga.out lines, which is checked here too."""
+    from gpuga_b200 import GA
+    kw = dict(seed=12345678, population_size=P, parent_number=P // 2, mutation_rate=0.2,
+              maximum_generation=gens + 3)
+    host = GA(e, **kw)
+    for _ in range(3):
+        host.step()
+    t0 = time.perf_counter()
+    host_lines = "".join(host.step() for _ in range(gens))
+    t_host = time.perf_counter() - t0
+    dev = GA(e, **kw)
+    dev.set_device_loop(True, 32)
+    dev.advance(3)
+    t0 = time.perf_counter()
+    dev_lines = dev.advance(gens)
+    t_dev = time.perf_counter() - t0
+    host.close()
+    dev.close()
+    return {"generations": gens, "host_loop_ms_per_gen": t_host * 1e3 / gens,
+            "device_loop_ms_per_gen": t_dev * 1e3 / gens, "identical_ga_out": host_lines == dev_lines}
 
 
 def cpu_baseline(data, budget_s: float) -> dict:

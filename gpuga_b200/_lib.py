@@ -68,6 +68,9 @@ PROTOTYPES = {
     "gpuga_ga_create_host": (i32, [i32, vp, vp, i32, i32, C.c_float, i32, C.c_uint, FITNESS_CB, vp, vp]),
     "gpuga_ga_step": (i32, [vp, C.c_char_p, i32]),
     "gpuga_ga_run": (i32, [vp, C.c_char_p]),
+    "gpuga_ga_advance": (i32, [vp, i32, C.c_char_p, C.c_longlong]),
+    "gpuga_ga_set_device_loop": (i32, [vp, i32, i32]),
+    "gpuga_ga_rank_device": (i32, [i32, i32, vp, vp, vp]),
     "gpuga_ga_state": (i32, [vp, vp, vp, vp]),
     "gpuga_ga_destroy": (i32, [vp]),
     "gpuga_potential_create": (i32, [i32, i32, vp]),

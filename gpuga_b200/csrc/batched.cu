@@ -13,17 +13,20 @@
 // fixed order, so a result never depends on what else shares the launch.
 //
 // Precision.  Pair, bond-order and three-body arithmetic is FP32 on CUDA cores
-// (accurate libdevice exp/pow/erfc/tanh, no fast-math); site energies and
+// (accurate libdevice exp/erfc/tanh, the bond-order power with a double-float
+// exponent (powf_dd.cuh), no fast-math); site energies and
 // virials are summed per atom in FP32 and across atoms in FP64; the loss and
 // normalisers are FP64.
 //
-// Geometry (unit vectors, distances, three-body cosines, RI Coulomb terms)
-// is parameter-independent and precomputed once (geometry.cu).
+// Geometry (unit vectors, distances, reverse-bond positions, RI Coulomb terms)
+// is parameter-independent and precomputed once (geometry.cu); three-body
+// cosines are dot products of the FP32 unit vectors, formed in registers.
 #include <algorithm>
 #include <cmath>
 #include <tuple>
 
 #include "engine.hpp"
+#include "powf_dd.cuh"
 
 namespace gpuga {
 
@@ -193,39 +196,44 @@ __device__ __forceinline__ void reduce_item(const WorkItem& it, int P, int Nc, d
   fold_item(it, P, Nc, red, res);
 }
 
-// Geometry of one configuration as a CTA sees it: in shared memory when the
-// work item was staged, otherwise the global arrays offset to the
-// configuration's first atom / bond.  Bond indices are local.
+// Geometry of one configuration as a CTA sees it.  Unstaged: the global CSR
+// arrays offset to the configuration's first atom / bond (bond j of local atom
+// il at boff[il] - bond0 + j).  Staged: a slot-major copy in shared memory
+// (bond j of atom il at j * Na + il, `stride` = Na), so that the lanes of a warp,
+// which hold consecutive atoms, read consecutive entries without bank conflicts.
 struct Geo {
-  const float4* g;     // [Bc] (unit vector, d)
-  const uint8_t* pt;   // [Bc] pair set
-  const int* rev;      // [Bc] reverse bond (global numbering; subtract bond0)
+  const float4* g;     // (unit vector, d)
+  const uint8_t* pt;   // pair set
+  const int* rev;      // slot * Na + atom of the reverse bond (force scratch position)
   const int* nn;       // [Na]
-  const int* boff;     // [Na] bond offset (global numbering; subtract bond0)
+  const int* boff;     // [Na] bond offset (global numbering; subtract bond0), unstaged only
   int bond0;
+  int stride;          // Na when staged (slot-major), 0 for the CSR arrays
+  __device__ __forceinline__ int base(int il) const { return stride ? il : boff[il] - bond0; }
+  __device__ __forceinline__ int step() const { return stride ? stride : 1; }
 };
 
-// Copies configuration c's geometry into shared memory with all threads of
-// the CTA (independent vector loads, then one barrier).
+// Copies configuration c's geometry into shared memory, slot-major with ZC
+// slots, with all threads of the CTA (independent loads, then one barrier).
+template <int ZC>
 __device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int Na, bool force, unsigned char* base) {
-  const int bond0 = S.off[atom0], bond1 = S.off[atom0 + Na];
-  const int Bc = bond1 - bond0;
+  const int n = ZC * Na;
   float4* sg = reinterpret_cast<float4*>(base);
-  int* snn = reinterpret_cast<int*>(sg + Bc);
-  int* sbo = snn + Na;
-  int* srev = sbo + Na;
-  uint8_t* spt = reinterpret_cast<uint8_t*>(srev + (force ? Bc : 0));
-  for (int k = threadIdx.x; k < Bc; k += blockDim.x) {
-    sg[k] = __ldg(&S.g32[bond0 + k]);
-    spt[k] = S.ptype[bond0 + k];
-    if (force) srev[k] = S.rev[bond0 + k];
+  int* snn = reinterpret_cast<int*>(sg + n);
+  int* srev = snn + Na;
+  uint8_t* spt = reinterpret_cast<uint8_t*>(srev + (force ? n : 0));
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const int j = t / Na, il = t - j * Na, i = atom0 + il;
+    if (j < S.NN[i]) {
+      const int b = S.off[i] + j;
+      sg[t] = __ldg(&S.g32[b]);
+      spt[t] = S.ptype[b];
+      if (force) srev[t] = S.rev_sm[b];
+    }
   }
-  for (int k = threadIdx.x; k < Na; k += blockDim.x) {
-    snn[k] = S.NN[atom0 + k];
-    sbo[k] = S.off[atom0 + k];
-  }
+  for (int k = threadIdx.x; k < Na; k += blockDim.x) snn[k] = S.NN[atom0 + k];
   __syncthreads();
-  return Geo{sg, spt, srev, snn, sbo, bond0};
+  return Geo{sg, spt, srev, snn, nullptr, 0, Na};
 }
 
 // One atom of the minimal Tersoff potential (minimal_tersoff.cu:122-405) for
@@ -238,22 +246,22 @@ __device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int N
 //   f_ij = 1/2 [ (A'_j - fc'_j sum_k T_k g_jk - m_j sum_k q_jk cos_jk) u_j + m_j sum_k q_jk u_k ]
 // with q_jk = beta (cos_jk - h) (S_j fc_k + T_k) and m_j = -2 fc_j / d_j.
 template <int ZC, int NT, bool FORCE>
-__device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C, int il, float* fsm, int G, int g,
-                                              float (&v)[6]) {
+__device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C, int il, int Na, float* fsm, int G,
+                                              int g, float (&v)[6]) {
   const int Z = geo.nn[il];
-  const int b0 = geo.boff[il] - geo.bond0;  // local
+  const int b0 = geo.base(il), bs = geo.step();  // bond j at b0 + j * bs
   float ux[ZC], uy[ZC], uz[ZC], dd[ZC];
   int st[ZC];
 #pragma unroll
   for (int j = 0; j < ZC; ++j) {
     st[j] = 0;
     if (j < Z) {
-      const float4 q = geo.g[b0 + j];
+      const float4 q = geo.g[b0 + j * bs];
       ux[j] = q.x;
       uy[j] = q.y;
       uz[j] = q.z;
       dd[j] = q.w;
-      if (NT == 2) st[j] = geo.pt[b0 + j];
+      if (NT == 2) st[j] = geo.pt[b0 + j * bs];
     } else {
       ux[j] = uy[j] = uz[j] = 0.f;
       dd[j] = 1.0f;
@@ -273,8 +281,22 @@ __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C,
     }
   }
   // pass B: bond order, site energy and the per-bond force scalars
-  // cos(theta_jik) = u_j . u_k from the FP32 unit vectors (as accurate as a stored FP32 cosine)
-  auto cosine = [&](int j, int k) { return fmaf(uz[j], uz[k], fmaf(uy[j], uy[k], ux[j] * ux[k])); };
+  // cos(theta_jik) = u_j . u_k from the FP32 unit vectors (as accurate as a stored FP32 cosine);
+  // the expression is symmetric bit for bit, so with up to 4 bonds the 6 distinct cosines are
+  // formed once and kept in registers for both passes
+  constexpr bool kSym = ZC == 4;
+  float cs[kSym ? ZC : 1][kSym ? ZC : 1];
+  if constexpr (kSym) {
+#pragma unroll
+    for (int j = 0; j < ZC; ++j)
+#pragma unroll
+      for (int k = j + 1; k < ZC; ++k)
+        cs[j][k] = cs[k][j] = fmaf(uz[j], uz[k], fmaf(uy[j], uy[k], ux[j] * ux[k]));
+  }
+  auto cosine = [&](int j, int k) {
+    if constexpr (kSym) return cs[j][k];
+    else return fmaf(uz[j], uz[k], fmaf(uy[j], uy[k], ux[j] * ux[k]));
+  };
   float Ap[ZC], Sb[ZC], Tb[ZC];
   float pe = 0.f;
 #pragma unroll
@@ -291,9 +313,9 @@ __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C,
       }
       float b = 1.f, bp = 0.f;
       if (!(zeta < 1.0e-16f)) {  // minimal_tersoff.cu:178-185
-        const float zn = powf(zeta, C.en);
+        const float zn = powf_dd(zeta, C.en);
         const float opz = 1.0f + zn;
-        b = powf(opz, C.mhon);
+        b = powf_dd(opz, C.mhon);
         bp = __fdividef(-0.5f * b * zn, opz * zeta);
       }
       const int s = NT == 2 ? st[j] : 0;
@@ -333,7 +355,9 @@ __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C,
       const float fy = fmaf(cu, uy[j], cv * Vy);
       const float fz = fmaf(cu, uz[j], cv * Vz);
       if (FORCE) {
-        const int bl = b0 + j;
+        // slot-major scratch [slot][atom][xyz][G]: the lanes of a warp (consecutive atoms,
+        // same slot) write consecutive words
+        const int bl = j * Na + il;
         fsm[(bl * 3 + 0) * G + g] = fx;
         fsm[(bl * 3 + 1) * G + g] = fy;
         fsm[(bl * 3 + 2) * G + g] = fz;
@@ -356,7 +380,7 @@ __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C,
 // that region.  Force items put the f_ij scratch first, the staged geometry
 // after it, and reuse the start of shared memory for the final fold.
 template <int ZC, int NT, bool FORCE, int BLK>
-__global__ void __launch_bounds__(BLK) tersoff_batched(const JobView* __restrict__ jobs,
+__global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_batched(const JobView* __restrict__ jobs,
                                                        const WorkItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int NW = BLK / 32;
@@ -383,13 +407,13 @@ __global__ void __launch_bounds__(BLK) tersoff_batched(const JobView* __restrict
     for (int k = 0; k < 7; ++k) red[k * BLK + threadIdx.x] = 0.0;
   }
   const Geo geo = item_staged(it)
-                      ? stage_geometry(S, atom0, Na, FORCE, smem + front)
-                      : Geo{S.g32 + bond0, S.ptype + bond0, S.rev + bond0, S.NN + atom0, S.off + atom0, bond0};
+                      ? stage_geometry<ZC>(S, atom0, Na, FORCE, smem + front)
+                      : Geo{S.g32 + bond0, S.ptype + bond0, S.rev_sm + bond0, S.NN + atom0, S.off + atom0, bond0, 0};
   for (int base = warp * A; base < Na; base += NW * A) {
     const int il = base + aslot;
     if (il < Na) {
       float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      const float pe = tersoff_atom<ZC, NT, FORCE>(geo, C, il, fsm, G, g, v);
+      const float pe = tersoff_atom<ZC, NT, FORCE>(geo, C, il, Na, fsm, G, g, v);
       if (!FORCE) {
         red[threadIdx.x] += (double)pe;
 #pragma unroll
@@ -409,10 +433,10 @@ __global__ void __launch_bounds__(BLK) tersoff_batched(const JobView* __restrict
     const int il = base + aslot;
     if (il < Na) {
       const int i = atom0 + il;
-      const int b0 = geo.boff[il] - bond0, Z = geo.nn[il];
+      const int b0 = geo.base(il), bs = geo.step(), Z = geo.nn[il];
       float Fx = 0.f, Fy = 0.f, Fz = 0.f;
       for (int j = 0; j < Z; ++j) {
-        const int bl = b0 + j, rl = geo.rev[b0 + j] - bond0;
+        const int bl = j * Na + il, rl = geo.rev[b0 + j * bs];
         Fx += fsm[(bl * 3 + 0) * G + g] - fsm[(rl * 3 + 0) * G + g];
         Fy += fsm[(bl * 3 + 1) * G + g] - fsm[(rl * 3 + 1) * G + g];
         Fz += fsm[(bl * 3 + 2) * G + g] - fsm[(rl * 3 + 2) * G + g];
@@ -479,6 +503,20 @@ __device__ __forceinline__ void ri_pair(const RIC& R, int t, float d, float4 w, 
     fd += -R.lr * fr + R.la * fa;
   }
 }
+
+// Compensated FP32 sum (Kahan): the running error c is subtracted from each
+// new term; value() is the sum in FP64.  Error about 2 eps sum|x| for any
+// order of terms, against (n - 1) eps sum|x| for a plain FP32 sum.
+struct KSum {
+  float s = 0.f, c = 0.f;
+  __device__ __forceinline__ void add(float x) {
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
 
 // NN2B value and derivative (nn2b.cu:49-78) for the lane's weights, held in
 // shared memory as float4 groups so that each 16-byte load feeds eight FMAs:
@@ -595,7 +633,10 @@ __global__ void __launch_bounds__(kBlock) pair_batched(const JobView* __restrict
     const int i = atom0 + il;
     const int bbeg = FORCE ? S.off[i] : S.half_off[i];
     const int bend = S.off[i + 1];
-    double Fx = 0, Fy = 0, Fz = 0;
+    // per-atom sums over the atom's pairs: compensated FP32 (Kahan), added to the
+    // FP64 accumulators once per atom -- a per-pair FP64 add would cost two
+    // FP32->FP64 conversions per term, which run at a fraction of the FP32 rate
+    KSum ks[FORCE ? 3 : 7];
 #pragma unroll 2
     for (int b = bbeg; b < bend; ++b) {
       const float4 q = __ldg(&S.g32[b]);
@@ -617,33 +658,36 @@ __global__ void __launch_bounds__(kBlock) pair_batched(const JobView* __restrict
         }
       }
       if (FORCE) {
-        Fx = fma((double)fd, (double)q.x, Fx);
-        Fy = fma((double)fd, (double)q.y, Fy);
-        Fz = fma((double)fd, (double)q.z, Fz);
+        ks[0].add(fd * q.x);
+        ks[1].add(fd * q.y);
+        ks[2].add(fd * q.z);
       } else {
         // unordered pair: full U and -r (x) r f2 with f2 = fd / d, i.e. -d fd u (x) u
-        acc[0] += (double)p2;
-        const float s = d * fd;
+        ks[0].add(p2);
+        const float s = -d * fd;
         const float sx = s * q.x, sy = s * q.y, sz = s * q.z;
-        acc[1] = fma(-(double)sx, (double)q.x, acc[1]);
-        acc[2] = fma(-(double)sy, (double)q.y, acc[2]);
-        acc[3] = fma(-(double)sz, (double)q.z, acc[3]);
-        acc[4] = fma(-(double)sx, (double)q.y, acc[4]);
-        acc[5] = fma(-(double)sy, (double)q.z, acc[5]);
-        acc[6] = fma(-(double)sz, (double)q.x, acc[6]);
+        ks[1].add(sx * q.x);
+        ks[2].add(sy * q.y);
+        ks[3].add(sz * q.z);
+        ks[4].add(sx * q.y);
+        ks[5].add(sy * q.z);
+        ks[6].add(sz * q.x);
       }
     }
     if (FORCE) {
-      const double dx = Fx - (double)S.force_ref[i];
-      const double dy = Fy - (double)S.force_ref[i + N];
-      const double dz = Fz - (double)S.force_ref[i + 2 * (size_t)N];
+      const double dx = ks[0].value() - (double)S.force_ref[i];
+      const double dy = ks[1].value() - (double)S.force_ref[i + N];
+      const double dz = ks[2].value() - (double)S.force_ref[i + 2 * (size_t)N];
       acc[7] += dx * dx + dy * dy + dz * dz;
       if (fdump && p < P) {
         const int Nf = S.N_force;
-        fdump[((size_t)p * 3 + 0) * Nf + i] = (float)Fx;
-        fdump[((size_t)p * 3 + 1) * Nf + i] = (float)Fy;
-        fdump[((size_t)p * 3 + 2) * Nf + i] = (float)Fz;
+        fdump[((size_t)p * 3 + 0) * Nf + i] = (float)ks[0].value();
+        fdump[((size_t)p * 3 + 1) * Nf + i] = (float)ks[1].value();
+        fdump[((size_t)p * 3 + 2) * Nf + i] = (float)ks[2].value();
       }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 7; ++k) acc[k] += ks[k].value();
     }
   }
   reduce_item(it, P, S.Nc, acc, smem, res);
@@ -701,8 +745,11 @@ __global__ void fitness_jobs(const JobView* __restrict__ jobs, const int2* __res
 // --------------------------------------------------------------------------- planning
 namespace {
 constexpr size_t kRedBytes = (size_t)kWarps * 32 * kResK * sizeof(double);
-constexpr size_t kForceSmemTarget = 96 * 1024;  // two CTAs per SM
-constexpr size_t kStageTarget = 110 * 1024;     // force scratch + staged geometry, two CTAs per SM
+// Force items with up to 4 bonds per atom: three 256-thread CTAs per SM (at most 85 registers
+// per thread, 74 KB of shared memory each) beat two CTAs with twice the individuals per item
+// (measured).  Larger register classes would spill under that bound and keep two CTAs per SM.
+size_t force_smem_target(int zc) { return zc == 4 ? 72 * 1024 : 96 * 1024; }
+size_t stage_target(int zc) { return zc == 4 ? 74 * 1024 : 110 * 1024; }  // force scratch + staged geometry
 // Energy/virial Tersoff items run in 128-thread CTAs (more resident warps per SM at ~115
 // registers per thread) and read their geometry through L1: staging it in shared memory
 // would cap the CTAs per SM without making the per-atom loads cheaper (measured).
@@ -724,7 +771,7 @@ DevView make_view(const DevSet& d) {
   v.NN = d.NN;
   v.off = d.off;
   v.half_off = d.half_off;
-  v.rev = d.rev;
+  v.rev_sm = d.rev_sm;
   v.ptype = d.ptype;
   v.g32 = d.g32;
   v.gri = d.gri;
@@ -848,19 +895,19 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
                   e->h_zmax[c]);
         return GPUGA_ERR_UNSUPPORTED;
       }
-      const size_t stage =
-          ((size_t)Bc * 16 + (size_t)Na * 8 + (force ? (size_t)Bc * 4 : 0) + (size_t)Bc + 15) & ~(size_t)15;
+      // slot-major staged geometry: zc slots per atom of (float4, pair set[, reverse position]) + counts
+      const size_t stage = ((size_t)zc * Na * (16 + 1 + (force ? 4 : 0)) + (size_t)Na * 4 + 15) & ~(size_t)15;
       if (force) {
-        const size_t per_ind = (size_t)Bc * 3 * sizeof(float);
-        while (G > 1 && per_ind * G > kForceSmemTarget) G >>= 1;
+        const size_t per_ind = (size_t)e->h_zmax[c] * Na * 3 * sizeof(float);  // slot-major, padded to max Z
+        while (G > 1 && per_ind * G > force_smem_target(zc)) G >>= 1;
         if (per_ind * G > kSmemMax) {
           set_error("configuration %d needs %zu bytes of force scratch per individual.", c, per_ind);
           return GPUGA_ERR_UNSUPPORTED;
         }
         // stage the geometry too when it fits beside the scratch of >= 4 individuals
         int Gs = G;
-        while (Gs > 4 && ((per_ind * Gs + 15) & ~(size_t)15) + stage > kStageTarget) Gs >>= 1;
-        if (((per_ind * Gs + 15) & ~(size_t)15) + stage <= kStageTarget) {
+        while (Gs > 4 && ((per_ind * Gs + 15) & ~(size_t)15) + stage > stage_target(zc)) Gs >>= 1;
+        if (((per_ind * Gs + 15) & ~(size_t)15) + stage <= stage_target(zc)) {
           G = Gs;
           staged = true;
         }
@@ -869,7 +916,7 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
       } else {
         // energy/virial items: per-lane FP64 sums of the 128-thread CTA, then (optionally) the geometry
         smem = (size_t)kBlockEV * kResK * sizeof(double);
-        if (kStageEV && stage <= kStageTarget) {
+        if (kStageEV && stage <= stage_target(zc)) {
           staged = true;
           smem += stage;
         }

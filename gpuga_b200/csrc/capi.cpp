@@ -17,6 +17,10 @@ struct gpuga_ga {
   gpuga_fitness_cb cb = nullptr;
   void* user = nullptr;
   std::vector<double> fit64;
+  DeviceGA* dga = nullptr;  // device-resident loop state, built on first use
+  int device_loop = 1;      // gpuga_ga_run on the device loop (engine GAs on the batched path)
+  int window = 32;          // generations per device-loop window
+  ~gpuga_ga() { device_ga_free(dga); }
 };
 
 namespace gpuga {
@@ -426,6 +430,14 @@ int gpuga_ga_step(gpuga_ga* g, char* line_out, int line_len) {
   return GPUGA_OK;
 }
 
+// ga.cu:150-158: screen echo of every tenth generation, numbered after the step
+static void echo_line(const gpuga_ga* g, const std::string& line) {
+  if (!g->e || !g->e->opt.verbose) return;
+  const size_t sp = line.find(' ');
+  const int gen = atoi(line.c_str()) + 1;
+  if (gen % 10 == 0) printf("%d%s", gen, line.substr(sp).c_str());
+}
+
 int gpuga_ga_run(gpuga_ga* g, const char* dir) {
   CHECK_ARG(g && dir, "gpuga_ga_run: null argument");
   std::string path = std::string(dir) + "/ga.out";
@@ -434,26 +446,62 @@ int gpuga_ga_run(gpuga_ga* g, const char* dir) {
     set_error("Failed to open %s.", path.c_str());
     return GPUGA_ERR_IO;
   }
-  std::string line;
-  while (g->g.generation < g->g.gp.maximum_generation) {
-    int s = g->g.step(&line);
-    if (s != GPUGA_OK) {
-      fclose(f);
-      return s;
+  if (g->e && g->device_loop && g->e->opt.path == GPUGA_PATH_BATCHED) {
+    int s = device_ga_advance(g->e, &g->g, &g->dga, g->g.gp.maximum_generation - g->g.generation, g->window,
+                              [&](const std::string& lines) {
+                                fputs(lines.c_str(), f);
+                                fflush(f);
+                                size_t a = 0;
+                                while (a < lines.size()) {
+                                  size_t b = lines.find('\n', a);
+                                  echo_line(g, lines.substr(a, b - a + 1));
+                                  a = b + 1;
+                                }
+                              });
+    fclose(f);
+    if (s != GPUGA_OK) return s;
+  } else {
+    std::string line;
+    while (g->g.generation < g->g.gp.maximum_generation) {
+      int s = g->g.step(&line);
+      if (s != GPUGA_OK) {
+        fclose(f);
+        return s;
+      }
+      fputs(line.c_str(), f);
+      fflush(f);
+      echo_line(g, line);
     }
-    fputs(line.c_str(), f);
-    fflush(f);
-    const int gen = g->g.generation;  // ga.cu:150-158: screen echo every 10 generations
-    if (g->e && g->e->opt.verbose && gen % 10 == 0) {
-      std::string l = line;
-      size_t sp = l.find(' ');
-      printf("%d%s", gen, l.substr(sp).c_str());
-    }
+    fclose(f);
   }
-  fclose(f);
   if (!g->e) return GPUGA_OK;
   gpuga_engine h{g->e};
   return gpuga_predict(&h, dir, g->g.population.data());
+}
+
+int gpuga_ga_set_device_loop(gpuga_ga* g, int enable, int window) {
+  CHECK_ARG(g, "gpuga_ga_set_device_loop: null GA");
+  CHECK_ARG(window >= 0, "gpuga_ga_set_device_loop: window must be >= 0");
+  g->device_loop = enable ? 1 : 0;
+  if (window > 0) g->window = window;
+  return GPUGA_OK;
+}
+
+int gpuga_ga_advance(gpuga_ga* g, int generations, char* lines_out, long long lines_len) {
+  CHECK_ARG(g, "gpuga_ga_advance: null GA");
+  CHECK_ARG(g->e, "gpuga_ga_advance: the device loop needs an engine GA (not a host-callback GA)");
+  CHECK_ARG(generations >= 0, "gpuga_ga_advance: generations must be >= 0");
+  std::string all;
+  int s = device_ga_advance(g->e, &g->g, &g->dga, generations, g->window,
+                            [&](const std::string& lines) { all += lines; });
+  if (s != GPUGA_OK) return s;
+  if (lines_out && lines_len > 0) snprintf(lines_out, (size_t)lines_len, "%s", all.c_str());
+  return GPUGA_OK;
+}
+
+int gpuga_ga_rank_device(int device, int P, const double* fitness, int* order, float* sorted) {
+  CHECK_ARG(fitness && order, "gpuga_ga_rank_device: null argument");
+  return device_rank(device, P, fitness, order, sorted);
 }
 
 int gpuga_ga_state(const gpuga_ga* g, int* generation, float* population_out, float* fitness_out) {

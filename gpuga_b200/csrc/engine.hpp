@@ -4,7 +4,8 @@
 //   configs  Na[Nc], Na_sum[Nc], cfg_zmax[Nc]
 //   atoms    type[N], r[3N] (SoA, FP32 as parsed), NN[N], off[N+1] (CSR into bonds),
 //            half_off[N] (first bond whose neighbor index is > i)
-//   bonds    nbr[B], rev[B] (reverse bond), ptype[B] (pair set / RI pair type),
+//   bonds    nbr[B], rev[B] (reverse bond), rev_sm[B] (the reverse bond's slot * Na + atom,
+//            local to the configuration), ptype[B] (pair set / RI pair type),
 //            g32[B] float4 (unit vector, d), g64[B] double4 (x,y,z,d),
 //            gri[B] float4 (RI geometry-only terms), image shift from the FP32 MIC
 //   targets  force_ref[3N], E_ref[Nc], W_ref[6Nc] (FP64 copies of the FP32 inputs)
@@ -15,8 +16,10 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "common.hpp"
@@ -41,6 +44,7 @@ struct DevSet {
   int* half_off = nullptr;
   int* nbr = nullptr;
   int* rev = nullptr;
+  int* rev_sm = nullptr;
   uint8_t* ptype = nullptr;
   float4* g32 = nullptr;
   double4* g64 = nullptr;
@@ -72,7 +76,7 @@ struct DevView {
   const int* NN;
   const int* off;
   const int* half_off;
-  const int* rev;
+  const int* rev_sm;
   const uint8_t* ptype;
   const float4* g32;
   const float4* gri;
@@ -229,6 +233,16 @@ int plan_get(Engine* e, int P, Plan** out);
 int plain_fitness(Engine* e, bool fp64, int P, const float* pop01, double* fitness, double* comps);
 int plain_find_force64(Engine* e, const double* params, double* F, double* W, double* pe);
 int plain_find_force32(Engine* e, const float* params, float* F, float* W, float* pe);
+
+// ga_device.cu: device-resident GA loop (selection, crossover, mutation on the GPU
+// from host-drawn plans); `sink` receives the ga.out lines of each finished window.
+struct GA;
+struct DeviceGA;
+int device_ga_advance(Engine* e, GA* ga, DeviceGA** state, int generations, int window,
+                      const std::function<void(const std::string&)>& sink);
+void device_ga_free(DeviceGA* s);
+// The GA's stable ascending order of FP32-rounded fitness values on the device: order[r] = i.
+int device_rank(int device, int P, const double* fitness, int* order, float* sorted);
 
 // engine.cu
 int engine_create(const PotentialSpec& spec, TrainingSet&& ts, const gpuga_options& opt, Engine** out);

@@ -66,21 +66,26 @@ void GA::sort_population() {
 }
 
 // ga.cu:138-147: "<generation> <best> <decoded elite...>" with %g
-std::string GA::output_line() const {
+std::string ga_output_line(int generation, float best, const float* elite01, const float* pmin,
+                           const float* pmax, int d) {
   std::string s;
   char buf[64];
-  snprintf(buf, sizeof buf, "%d %g ", generation, fitness[0]);
+  snprintf(buf, sizeof buf, "%d %g ", generation, best);
   s += buf;
   for (int m = 0; m < d; ++m) {
     volatile float a = pmin[m];
     volatile float b = pmax[m] - a;
-    volatile float bx = b * population[m];
+    volatile float bx = b * elite01[m];
     float v = a + bx;
     snprintf(buf, sizeof buf, "%g ", v);
     s += buf;
   }
   s += "\n";
   return s;
+}
+
+std::string GA::output_line() const {
+  return ga_output_line(generation, fitness[0], population.data(), pmin.data(), pmax.data(), d);
 }
 
 // ga.cu:200-212
@@ -97,14 +102,57 @@ int GA::get_a_parent() {
   return parent;
 }
 
-// ga.cu:161-186
-void GA::crossover() {
+int GA::mutation_count(int g) const {
+  // ga.cu:190-192: rate in double stored to float, count rounded from float
+  float rate_n = gp.mutation_rate * (1.0 - float(g) / gp.maximum_generation);
+  int m = gp.population_size * d;
+  return (int)std::round(m * rate_n);
+}
+
+// ga.cu:161-198, draws only.  Crossover (161-186): parents by rank, redrawn
+// until they differ, point U{1, d-1}.  Mutation (188-198): the reference writes
+// population[r1(rng)] = r2(rng) and is compiled as C++14, where GCC evaluates
+// the index first; the order is explicit here.
+void GA::draw_plan(int g, GenPlan* plan) {
+  plan->pairs.resize((size_t)child_number / 2 * 3);
   for (int m = 0; m < child_number; m += 2) {
     int parent_1 = get_a_parent();
     int parent_2 = get_a_parent();
     while (parent_2 == parent_1) parent_2 = get_a_parent();
     std::uniform_int_distribution<int> r1(1, d - 1);
     int crossover_point = r1(rng);
+    int* q = &plan->pairs[(size_t)m / 2 * 3];
+    q[0] = parent_1;
+    q[1] = parent_2;
+    q[2] = crossover_point;
+  }
+  const int m = gp.population_size * d;
+  const int count = mutation_count(g);
+  std::vector<int> idx(count);
+  std::vector<float> val(count);
+  for (int n = 0; n < count; ++n) {
+    std::uniform_int_distribution<int> r1(d, m - 1);
+    std::uniform_real_distribution<float> r2(0, 1);
+    idx[n] = r1(rng);
+    val[n] = r2(rng);
+  }
+  // fold repeated genes: walking backwards, the first write seen is the one that stays
+  if (stamp.size() != (size_t)m) stamp.assign(m, -1);
+  ++stamp_tag;
+  plan->mut_idx.clear();
+  plan->mut_val.clear();
+  for (int n = count - 1; n >= 0; --n) {
+    if (stamp[idx[n]] == stamp_tag) continue;
+    stamp[idx[n]] = stamp_tag;
+    plan->mut_idx.push_back(idx[n]);
+    plan->mut_val.push_back(val[n]);
+  }
+}
+
+void GA::apply_plan(const GenPlan& plan) {
+  for (int m = 0; m < child_number; m += 2) {
+    const int* q = &plan.pairs[(size_t)m / 2 * 3];
+    const int parent_1 = q[0], parent_2 = q[1], crossover_point = q[2];
     int child_1 = gp.parent_number + m;
     int child_2 = child_1 + 1;
     for (int n = 0; n < crossover_point; ++n) {
@@ -116,21 +164,7 @@ void GA::crossover() {
       population[(size_t)child_2 * d + n] = population[(size_t)parent_1 * d + n];
     }
   }
-}
-
-// ga.cu:188-198.  The reference writes population[r1(rng)] = r2(rng) and is
-// compiled as C++14, where GCC evaluates the index first; the order is explicit here.
-void GA::mutation() {
-  float rate_n = gp.mutation_rate * (1.0 - float(generation) / gp.maximum_generation);
-  int m = gp.population_size * d;
-  int number_of_mutations = (int)std::round(m * rate_n);
-  for (int n = 0; n < number_of_mutations; ++n) {
-    std::uniform_int_distribution<int> r1(d, m - 1);
-    std::uniform_real_distribution<float> r2(0, 1);
-    const int idx = r1(rng);
-    const float val = r2(rng);
-    population[idx] = val;
-  }
+  for (size_t n = 0; n < plan.mut_idx.size(); ++n) population[plan.mut_idx[n]] = plan.mut_val[n];
 }
 
 int GA::step(std::string* line) {
@@ -140,8 +174,9 @@ int GA::step(std::string* line) {
   sort_population();
   std::string l = output_line();
   if (line) *line = l;
-  crossover();
-  mutation();
+  GenPlan plan;
+  draw_plan(generation, &plan);
+  apply_plan(plan);
   ++generation;
   return GPUGA_OK;
 }

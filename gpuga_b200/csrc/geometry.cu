@@ -9,8 +9,8 @@
 // From the list the engine derives, once per training set, everything that
 // does not depend on the potential parameters: FP64 bond vectors for the
 // image the FP32 rule picked, unit vectors and distances in FP32, reverse-bond
-// indices, three-body cosines and the fixed-damping Coulomb terms of the RI
-// potential.
+// indices (and their positions in the batched force scratch) and the
+// fixed-damping Coulomb terms of the RI potential.
 #include <cmath>
 #include <numeric>
 
@@ -176,6 +176,20 @@ __global__ void bond_geometry(int N, const int* __restrict__ atom_cfg, const flo
   half_off[i] = hstart;
 }
 
+// Position of each bond's reverse in the batched force kernel's slot-major
+// scratch of its configuration: slot * Na + atom, both local to the configuration.
+__global__ void reverse_slots(int N, const int* __restrict__ atom_cfg, const int* __restrict__ Na,
+                              const int* __restrict__ Na_sum, const int* __restrict__ off,
+                              const int* __restrict__ nbr, const int* __restrict__ rev, int* __restrict__ rev_sm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int c = atom_cfg[i], atom0 = Na_sum[c], na = Na[c];
+  for (int b = off[i]; b < off[i + 1]; ++b) {
+    const int j = nbr[b];
+    rev_sm[b] = (rev[b] - off[j]) * na + (j - atom0);
+  }
+}
+
 // Bond geometry for lists in the reference layout NL[k*N + i]: the FP32 rule
 // picks the image, the vector is then evaluated in FP64; rev holds the slot of
 // the reverse bond (slot 0 of the neighbor when absent, minimal_tersoff.cu:368).
@@ -293,6 +307,9 @@ int build_geometry(Engine* e) {
   bond_geometry<<<(N + 127) / 128, 128, 0, st>>>(N, d_atom_cfg, d.h, d.r, d.type, d.off, d.nbr, img,
                                                  d.potential_type, d.num_types, rc_fixed, d.g64, d.g32, d.gri, d.rev,
                                                  d.half_off, d.ptype);
+  GPUGA_CUDA(cudaGetLastError());
+  GPUGA_TRY(e->alloc(&d.rev_sm, std::max(B, 1)));
+  reverse_slots<<<(N + 127) / 128, 128, 0, st>>>(N, d_atom_cfg, d.Na, d.Na_sum, d.off, d.nbr, d.rev, d.rev_sm);
   GPUGA_CUDA(cudaGetLastError());
 
   GPUGA_CUDA(cudaStreamSynchronize(st));

@@ -259,6 +259,15 @@ class GA:
     def run(self, input_dir: str) -> None:
         check(_lib.load().gpuga_ga_run(self._h, input_dir.encode()))
 
+    def advance(self, generations: int) -> str:
+        """`generations` generations on the device-resident loop; returns their ga.out lines."""
+        buf = C.create_string_buffer(generations * (64 + 20 * self.num_vars) + 1)
+        check(_lib.load().gpuga_ga_advance(self._h, generations, buf, len(buf)))
+        return buf.value.decode()
+
+    def set_device_loop(self, enable: bool, window: int = 0) -> None:
+        check(_lib.load().gpuga_ga_set_device_loop(self._h, int(enable), window))
+
     def state(self, population_size: int):
         gen = C.c_int()
         pop = np.zeros((population_size, self.num_vars), np.float32)

@@ -163,8 +163,24 @@ int gpuga_ga_create_host(int num_vars, const float* pmin, const float* pmax, int
 /* One generation: evaluate, sort, output line, crossover, mutation (ga.cu:82-88).
  * line_out (may be NULL) receives the ga.out line for this generation. */
 int gpuga_ga_step(gpuga_ga* g, char* line_out, int line_len);
-/* Runs all remaining generations writing <dir>/ga.out, then predict() (ga.cu:73-92). */
+/* Runs all remaining generations writing <dir>/ga.out, then predict() (ga.cu:73-92).  Engine GAs on
+ * the batched path run the device-resident loop (gpuga_ga_advance) unless it was switched off. */
 int gpuga_ga_run(gpuga_ga* g, const char* dir);
+/* Device-resident GA loop (replaces the host round trip of every GA::compute generation, ga.cu:78-92):
+ * selection (the stable insertion sort of ga.cu:105-137, NaN included), crossover and mutation run on
+ * the GPU behind the batched fitness launches, from random choices the host draws from the same
+ * std::mt19937 stream in the reference's order, `window` generations per batch (one CUDA graph per
+ * generation, replayed).  The result -- ga.out lines, population, fitness, random stream -- is the same
+ * as `generations` calls of gpuga_ga_step.  Engine GAs on the batched path only; populations up to
+ * 49152.  lines_out (may be NULL) receives the concatenated ga.out lines, truncated to lines_len. */
+int gpuga_ga_advance(gpuga_ga* g, int generations, char* lines_out, long long lines_len);
+/* enable: whether gpuga_ga_run uses the device loop (default 1); window > 0 sets generations per batch
+ * (default 32), 0 keeps it. */
+int gpuga_ga_set_device_loop(gpuga_ga* g, int enable, int window);
+/* The device loop's selection order on its own: fitness double[P] is rounded to FP32 and ordered as the
+ * reference's stable insertion sort orders it (ga.cu:105-119; a NaN keeps its place and no value moves
+ * past it).  order[r] = index of the r-th individual; sorted (may be NULL) float[P]. */
+int gpuga_ga_rank_device(int device, int P, const double* fitness, int* order, float* sorted);
 /* population_out float[P*num_vars] (sorted after the last step), fitness_out float[P] */
 int gpuga_ga_state(const gpuga_ga* g, int* generation, float* population_out, float* fitness_out);
 int gpuga_ga_destroy(gpuga_ga* g);
