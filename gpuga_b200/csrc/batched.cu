@@ -160,13 +160,15 @@ __device__ __forceinline__ void cutoff_fn(float r1, float r2, float pf, float d,
 }
 
 // WorkItem::G packs the individuals per item (bits 0-7), whether the item's
-// geometry is staged in shared memory (bit 8) and the byte size of the force
-// scratch that precedes the staged geometry, in 16-byte units (bits 9-23).
+// geometry is staged in shared memory (bit 8), the byte size of the force
+// scratch that precedes the staged geometry, in 16-byte units (bits 9-23), and
+// whether the force scratch lives in global memory instead (bit 24).
 __host__ __device__ __forceinline__ int item_G(const WorkItem& it) { return it.G & 0xff; }
 __host__ __device__ __forceinline__ bool item_staged(const WorkItem& it) { return (it.G >> 8) & 1; }
 __host__ __device__ __forceinline__ size_t item_fbytes(const WorkItem& it) { return (size_t)((it.G >> 9) & 0x7fff) * 16; }
-__host__ __device__ __forceinline__ int pack_G(int G, bool staged, size_t fbytes) {
-  return G | (staged ? 1 << 8 : 0) | (int)(((fbytes + 15) / 16) << 9);
+__host__ __device__ __forceinline__ bool item_global(const WorkItem& it) { return (it.G >> 24) & 1; }
+__host__ __device__ __forceinline__ int pack_G(int G, bool staged, size_t fbytes, bool global = false) {
+  return G | (staged ? 1 << 8 : 0) | (int)(((fbytes + 15) / 16) << 9) | (global ? 1 << 24 : 0);
 }
 
 // Fixed-order fold of per-lane partial sums held in shared memory as
@@ -399,7 +401,9 @@ __global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_ba
   load_tersoff(kc, C);
   const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
   const int bond0 = S.off[atom0];
-  float* fsm = reinterpret_cast<float*>(smem);
+  // force scratch: shared memory, or for configurations too large for it the item's own
+  // region of global memory (visible to the whole CTA after __syncthreads as well)
+  float* fsm = FORCE && item_global(it) ? J.gscratch + (size_t)it.gofs * 64 : reinterpret_cast<float*>(smem);
   double* red = reinterpret_cast<double*>(smem);
   const size_t front = FORCE ? item_fbytes(it) : (size_t)BLK * kResK * sizeof(double);
   if (!FORCE) {
@@ -542,27 +546,32 @@ struct NNSmem {
   }
 };
 
-template <int NMAX>
-__device__ __forceinline__ void nn_pair(const float* __restrict__ wsm, int lane, int n, float d, float& p2,
-                                        float& f2) {
+// NP pairs of the same lane at once: every weight loaded from shared memory
+// feeds the NP pairs (the hidden-to-hidden loads, not the FMAs, bound a
+// single pair).  Each pair's arithmetic is the same sequence as for NP = 1.
+template <int NMAX, int NP>
+__device__ __forceinline__ void nn_pairs(const float* __restrict__ wsm, int lane, int n, const float (&d)[NP],
+                                         float (&p2)[NP], float (&f2)[NP]) {
   constexpr int Q = NMAX / 4;
   const float4* W1 = reinterpret_cast<const float4*>(wsm);
   const float4* V = W1 + NMAX * Q * 32;
   const float b2 = wsm[(size_t)(NMAX * Q * 32 + 4 * Q * 32) * 4 + lane];
-  float x1[NMAX], y1[NMAX];
+  float x1[NP][NMAX], y1[NP][NMAX];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const float4 w0 = V[(0 * Q + q) * 32 + lane];
     const float4 b0 = V[(1 * Q + q) * 32 + lane];
     const float w0c[4] = {w0.x, w0.y, w0.z, w0.w}, b0c[4] = {b0.x, b0.y, b0.z, b0.w};
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      x1[4 * q + c] = tanhf(w0c[c] * d - b0c[c]);
-      y1[4 * q + c] = (1.0f - x1[4 * q + c] * x1[4 * q + c]) * w0c[c];
-    }
+    for (int u = 0; u < NP; ++u)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        x1[u][4 * q + c] = tanhf(w0c[c] * d[u] - b0c[c]);
+        y1[u][4 * q + c] = (1.0f - x1[u][4 * q + c] * x1[u][4 * q + c]) * w0c[c];
+      }
   }
-  p2 = 0.f;
-  f2 = 0.f;
+#pragma unroll
+  for (int u = 0; u < NP; ++u) p2[u] = f2[u] = 0.f;
   const int qa_end = (n + 3) >> 2;
   for (int qa = 0; qa < qa_end; ++qa) {
     const float4 b1 = V[(2 * Q + qa) * 32 + lane];
@@ -572,31 +581,42 @@ __device__ __forceinline__ void nn_pair(const float* __restrict__ wsm, int lane,
     for (int c = 0; c < 4; ++c) {
       const int a = 4 * qa + c;
       if (a < n) {
-        float x2 = 0.f, y2 = 0.f;
+        float x2[NP], y2[NP];
+#pragma unroll
+        for (int u = 0; u < NP; ++u) x2[u] = y2[u] = 0.f;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
           const float4 w = W1[(a * Q + q) * 32 + lane];
-          x2 = fmaf(w.x, x1[4 * q], x2);
-          y2 = fmaf(w.x, y1[4 * q], y2);
-          x2 = fmaf(w.y, x1[4 * q + 1], x2);
-          y2 = fmaf(w.y, y1[4 * q + 1], y2);
-          x2 = fmaf(w.z, x1[4 * q + 2], x2);
-          y2 = fmaf(w.z, y1[4 * q + 2], y2);
-          x2 = fmaf(w.w, x1[4 * q + 3], x2);
-          y2 = fmaf(w.w, y1[4 * q + 3], y2);
+#pragma unroll
+          for (int u = 0; u < NP; ++u) {
+            x2[u] = fmaf(w.x, x1[u][4 * q], x2[u]);
+            y2[u] = fmaf(w.x, y1[u][4 * q], y2[u]);
+            x2[u] = fmaf(w.y, x1[u][4 * q + 1], x2[u]);
+            y2[u] = fmaf(w.y, y1[u][4 * q + 1], y2[u]);
+            x2[u] = fmaf(w.z, x1[u][4 * q + 2], x2[u]);
+            y2[u] = fmaf(w.z, y1[u][4 * q + 2], y2[u]);
+            x2[u] = fmaf(w.w, x1[u][4 * q + 3], x2[u]);
+            y2[u] = fmaf(w.w, y1[u][4 * q + 3], y2[u]);
+          }
         }
-        x2 = tanhf(x2 - b1c[c]);
-        y2 *= 1.0f - x2 * x2;
-        p2 = fmaf(w2c[c], x2, p2);
-        f2 = fmaf(w2c[c], y2, f2);
+#pragma unroll
+        for (int u = 0; u < NP; ++u) {
+          const float x2t = tanhf(x2[u] - b1c[c]);
+          const float y2t = y2[u] * (1.0f - x2t * x2t);
+          p2[u] = fmaf(w2c[c], x2t, p2[u]);
+          f2[u] = fmaf(w2c[c], y2t, f2[u]);
+        }
       }
     }
   }
-  p2 -= b2;
+#pragma unroll
+  for (int u = 0; u < NP; ++u) p2[u] -= b2;
 }
 
+// RI: three CTAs per SM (at most 85 registers); NN2B: two (128 registers, two pairs per
+// weight load) -- each measured faster than the unbounded register allocation.
 template <int KIND, int NMAX, bool FORCE>
-__global__ void __launch_bounds__(kBlock) pair_batched(const JobView* __restrict__ jobs,
+__global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const JobView* __restrict__ jobs,
                                                        const WorkItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem[];
   const WorkItem it = items[blockIdx.x];
@@ -637,26 +657,7 @@ __global__ void __launch_bounds__(kBlock) pair_batched(const JobView* __restrict
     // FP64 accumulators once per atom -- a per-pair FP64 add would cost two
     // FP32->FP64 conversions per term, which run at a fraction of the FP32 rate
     KSum ks[FORCE ? 3 : 7];
-#pragma unroll 2
-    for (int b = bbeg; b < bend; ++b) {
-      const float4 q = __ldg(&S.g32[b]);
-      const float d = q.w;
-      float p2, fd;
-      if (KIND == 1) {
-        ri_pair(R, S.ptype[b], d, __ldg(&S.gri[b]), p2, fd);
-      } else {
-        float f2raw;
-        nn_pair<NMAX>(wsm, lane, nn, d, p2, f2raw);
-        float fc, fcp;
-        cutoff_fn(tp.r1, tp.r2, tp.pf, d, fc, fcp);
-        if (tp.consistent) {
-          fd = f2raw * fc + p2 * fcp;
-          p2 *= fc;
-        } else {  // nn2b.cu:147-148: p2 is tapered before it enters the force
-          p2 *= fc;
-          fd = f2raw * fc + p2 * fcp;
-        }
-      }
+    auto consume = [&](const float4& q, float p2, float fd) {
       if (FORCE) {
         ks[0].add(fd * q.x);
         ks[1].add(fd * q.y);
@@ -664,7 +665,7 @@ __global__ void __launch_bounds__(kBlock) pair_batched(const JobView* __restrict
       } else {
         // unordered pair: full U and -r (x) r f2 with f2 = fd / d, i.e. -d fd u (x) u
         ks[0].add(p2);
-        const float s = -d * fd;
+        const float s = -q.w * fd;
         const float sx = s * q.x, sy = s * q.y, sz = s * q.z;
         ks[1].add(sx * q.x);
         ks[2].add(sy * q.y);
@@ -672,6 +673,44 @@ __global__ void __launch_bounds__(kBlock) pair_batched(const JobView* __restrict
         ks[4].add(sx * q.y);
         ks[5].add(sy * q.z);
         ks[6].add(sz * q.x);
+      }
+    };
+    if constexpr (KIND == 1) {
+#pragma unroll 2
+      for (int b = bbeg; b < bend; ++b) {
+        const float4 q = __ldg(&S.g32[b]);
+        float p2, fd;
+        ri_pair(R, S.ptype[b], q.w, __ldg(&S.gri[b]), p2, fd);
+        consume(q, p2, fd);
+      }
+    } else {
+      // two pairs per weight load up to 16 neurons (registers allow it), one above
+      constexpr int NP = NMAX <= 16 ? 2 : 1;
+      for (int b = bbeg; b < bend; b += NP) {
+        float4 q[NP];
+        float d[NP], p2[NP], f2raw[NP];
+#pragma unroll
+        for (int u = 0; u < NP; ++u) {
+          q[u] = __ldg(&S.g32[min(b + u, bend - 1)]);
+          d[u] = q[u].w;
+        }
+        nn_pairs<NMAX, NP>(wsm, lane, nn, d, p2, f2raw);
+#pragma unroll
+        for (int u = 0; u < NP; ++u) {
+          if (b + u < bend) {
+            float fc, fcp, fd;
+            cutoff_fn(tp.r1, tp.r2, tp.pf, d[u], fc, fcp);
+            float pu = p2[u];
+            if (tp.consistent) {
+              fd = f2raw[u] * fc + pu * fcp;
+              pu *= fc;
+            } else {  // nn2b.cu:147-148: p2 is tapered before it enters the force
+              pu *= fc;
+              fd = f2raw[u] * fc + pu * fcp;
+            }
+            consume(q[u], pu, fd);
+          }
+        }
       }
     }
     if (FORCE) {
@@ -800,6 +839,7 @@ JobView make_job_view(const Engine* e, const Plan* plan) {
   j.weights = plan->d_weights;
   j.res = plan->d_res;
   j.fdump = plan->dump ? plan->d_fdump : nullptr;
+  j.gscratch = plan->d_gscratch;
   j.E_ref = d.E_ref;
   j.W_ref = d.W_ref;
   j.nF = d.norm_force;
@@ -851,7 +891,8 @@ struct LaunchKey {
 //     RI:      25 flops + 2 transcendentals per pair (Morse included on average)
 //     NN2B:    4n^2 + 13n + 10 flops + 2n tanh per pair
 int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<ItemSpec>>& groups,
-              std::map<LaunchKey, size_t>& smem_need) {
+              std::map<LaunchKey, size_t>& smem_need, size_t* gscratch_floats) {
+  *gscratch_floats = 0;
   const DevSet& d = e->d;
   const TrainingSet& ts = e->ts;
   const bool tersoff = d.potential_type == 1 || d.potential_type == 2;
@@ -886,8 +927,8 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
     const long long Bc = (long long)e->h_off[ts.Na_sum[c] + Na] - e->h_off[ts.Na_sum[c]];
     int zc = 0, G = 32;
     size_t smem = kRedBytes;
-    bool staged = false;
-    size_t fbytes = 0;
+    bool staged = false, global = false;
+    size_t fbytes = 0, item_floats = 0;
     if (kind == 0) {
       zc = zclass_of(e->h_zmax[c]);
       if (zc == 0) {
@@ -897,13 +938,14 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
       }
       // slot-major staged geometry: zc slots per atom of (float4, pair set[, reverse position]) + counts
       const size_t stage = ((size_t)zc * Na * (16 + 1 + (force ? 4 : 0)) + (size_t)Na * 4 + 15) & ~(size_t)15;
-      if (force) {
-        const size_t per_ind = (size_t)e->h_zmax[c] * Na * 3 * sizeof(float);  // slot-major, padded to max Z
+      const size_t per_ind = (size_t)e->h_zmax[c] * Na * 3 * sizeof(float);  // slot-major, padded to max Z
+      if (force && per_ind > force_smem_target(zc)) {
+        // not even one individual's scratch fits: 32 individuals per item (lane = individual,
+        // coalesced scratch rows) with the scratch in global memory
+        global = true;
+        item_floats = ((per_ind / sizeof(float)) * 32 + 63) & ~(size_t)63;
+      } else if (force) {
         while (G > 1 && per_ind * G > force_smem_target(zc)) G >>= 1;
-        if (per_ind * G > kSmemMax) {
-          set_error("configuration %d needs %zu bytes of force scratch per individual.", c, per_ind);
-          return GPUGA_ERR_UNSUPPORTED;
-        }
         // stage the geometry too when it fits beside the scratch of >= 4 individuals
         int Gs = G;
         while (Gs > 4 && ((per_ind * Gs + 15) & ~(size_t)15) + stage > stage_target(zc)) Gs >>= 1;
@@ -935,7 +977,17 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
     }
     for (int p0 = 0; p0 < P; p0 += G) {
       const int cnt = std::min(G, P - p0);
-      groups[key].push_back({WorkItem{c, p0, pack_G(G, staged, fbytes), job}, cf * cnt, (double)Na * cnt, cf * cnt, cs * cnt});
+      int gofs = 0;
+      if (global) {
+        if (*gscratch_floats / 64 > (size_t)INT32_MAX) {
+          set_error("global force scratch exceeds the addressable size.");
+          return GPUGA_ERR_UNSUPPORTED;
+        }
+        gofs = (int)(*gscratch_floats / 64);
+        *gscratch_floats += item_floats;
+      }
+      groups[key].push_back(
+          {WorkItem{c, p0, pack_G(G, staged, fbytes, global), job, gofs}, cf * cnt, (double)Na * cnt, cf * cnt, cs * cnt});
     }
   }
   return GPUGA_OK;
@@ -1005,8 +1057,15 @@ int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSe
   std::vector<int2> indmap;
   ls->jobs.clear();
   for (size_t j = 0; j < jobs.size(); ++j) {
-    GPUGA_TRY(job_items(jobs[j].first, jobs[j].second->P, (int)j, groups, smem_need));
-    ls->jobs.push_back(make_job_view(jobs[j].first, jobs[j].second));
+    Engine* e = jobs[j].first;
+    Plan* plan = jobs[j].second;
+    size_t need = 0;
+    GPUGA_TRY(job_items(e, plan->P, (int)j, groups, smem_need, &need));
+    if (need > plan->gscratch_floats) {
+      GPUGA_TRY(e->alloc(&plan->d_gscratch, need));
+      plan->gscratch_floats = need;
+    }
+    ls->jobs.push_back(make_job_view(e, plan));
     for (int p = 0; p < jobs[j].second->P; ++p) indmap.push_back(make_int2((int)j, p));
   }
   std::vector<WorkItem> all;

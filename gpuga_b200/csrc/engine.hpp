@@ -64,8 +64,10 @@ struct DevSet {
 struct WorkItem {
   int config;
   int p0;
-  int G;    // individuals per item (power of two <= 32); lanes = G individuals x (32/G) atoms
-  int job;  // row of the launch set's job table
+  int G;     // individuals per item (power of two <= 32); lanes = G individuals x (32/G) atoms
+  int job;   // row of the launch set's job table
+  int gofs;  // force items too large for shared memory: offset of the item's f_ij scratch in the
+             // job's global scratch, in units of 64 floats
 };
 
 // Read-only training-set view the batched kernels use.
@@ -101,6 +103,7 @@ struct JobView {
   float* weights;        // NN2B [num_vars][Pstride]
   double* res;           // [P][Nc][kResK]
   float* fdump;          // optional [P][3][N_force]
+  float* gscratch;       // f_ij scratch of the force items that do not fit shared memory
   const double* E_ref;
   const double* W_ref;
   double nF, nE, nW;
@@ -154,6 +157,8 @@ struct Plan {
   float* h_pop = nullptr;      // pinned
   double* h_fit = nullptr;     // pinned [4P]: fitness + 3 components
   float* d_fdump = nullptr;    // optional per-atom forces of force configs [P][3][N_force]
+  float* d_gscratch = nullptr; // f_ij scratch of force items too large for shared memory
+  size_t gscratch_floats = 0;
   bool dump = false;           // pass d_fdump to the kernels (eager launches only)
   cudaGraphExec_t graph = nullptr;
   std::unique_ptr<LaunchSet> ls;

@@ -11,8 +11,10 @@
 // image the FP32 rule picked, unit vectors and distances in FP32, reverse-bond
 // indices (and their positions in the batched force scratch) and the
 // fixed-damping Coulomb terms of the RI potential.
+#include <algorithm>
 #include <cmath>
 #include <numeric>
+#include <vector>
 
 #include "engine.hpp"
 
@@ -51,14 +53,28 @@ __device__ __forceinline__ void mic32(const float* h, float& x, float& y, float&
   z = dot3<MODE>(h[6], sx, h[7], sy, h[8], sz);
 }
 
+// The reference's pair test (neighbor.cu:51-60): FP32 difference, nearest
+// image, strict d^2 < rc^2.  Returns the image shift removed.
+template <int MODE>
+__device__ __forceinline__ bool pair_within(const float* hh, float rc2, const float* __restrict__ r, int N,
+                                            float x1, float y1, float z1, int n2, float& ix, float& iy, float& iz) {
+  float x12 = __fsub_rn(r[n2], x1);
+  float y12 = __fsub_rn(r[n2 + N], y1);
+  float z12 = __fsub_rn(r[n2 + 2 * (size_t)N], z1);
+  mic32<MODE>(hh, x12, y12, z12, ix, iy, iz);
+  return dot3<MODE>(x12, x12, y12, y12, z12, z12) < rc2;
+}
+
 // One CTA per configuration, atoms strided over the threads.  Pass 0 counts,
-// pass 1 writes the CSR list and the image shifts.
+// pass 1 writes the CSR list and the image shifts.  Configurations listed in
+// `skip` (cell-list configurations) are left to neighbor_cells.
 template <int MODE, bool FILL>
 __global__ void neighbor_scan(int N, const int* __restrict__ Na, const int* __restrict__ Na_sum,
                               float rc2, const float* __restrict__ box, const float* __restrict__ r,
                               int* __restrict__ NN, const int* __restrict__ off, int* __restrict__ nbr,
-                              float* __restrict__ img) {
+                              float* __restrict__ img, const uint8_t* __restrict__ skip) {
   const int c = blockIdx.x;
+  if (skip && skip[c]) return;
   const int n_begin = Na_sum[c], n_end = n_begin + Na[c];
   const float* h = box + 18 * (size_t)c;
   float hh[18];
@@ -70,13 +86,8 @@ __global__ void neighbor_scan(int N, const int* __restrict__ Na, const int* __re
     int base = FILL ? off[n1] : 0;
     for (int n2 = n_begin; n2 < n_end; ++n2) {
       if (n2 == n1) continue;
-      float x12 = __fsub_rn(r[n2], x1);
-      float y12 = __fsub_rn(r[n2 + N], y1);
-      float z12 = __fsub_rn(r[n2 + 2 * (size_t)N], z1);
       float ix, iy, iz;
-      mic32<MODE>(hh, x12, y12, z12, ix, iy, iz);
-      const float d2 = dot3<MODE>(x12, x12, y12, y12, z12, z12);
-      if (d2 < rc2) {
+      if (pair_within<MODE>(hh, rc2, r, N, x1, y1, z1, n2, ix, iy, iz)) {
         if (FILL) {
           nbr[base + count] = n2;
           img[3 * (size_t)(base + count) + 0] = ix;
@@ -87,6 +98,74 @@ __global__ void neighbor_scan(int N, const int* __restrict__ Na, const int* __re
       }
     }
     if (!FILL) NN[n1] = count;
+  }
+}
+
+// Cell-list build for large configurations: one thread per atom visits the 27
+// cells around its own (cell widths >= rc, >= 3 cells per direction, so every
+// pair within rc is visited exactly once), applies the same FP32 pair test and,
+// in the fill pass, sorts its neighbors ascending -- the list is then the
+// reference's, bit for bit, in O(N) instead of O(Na^2) per configuration.
+//   atoms[k]: atoms handled here; acell[k] = (cell x, y, z, grid row) of atoms[k];
+//   grid[g] = (nx, ny, nz, first cell); cell_atoms[cell_start[cell] .. cell_start[cell + 1]).
+template <int MODE, bool FILL>
+__global__ void neighbor_cells(int N, int n_atoms, const int* __restrict__ atoms, const int4* __restrict__ acell,
+                               const int4* __restrict__ grid, const int* __restrict__ grid_cfg,
+                               const int* __restrict__ cell_start, const int* __restrict__ cell_atoms, float rc2,
+                               const float* __restrict__ box, const float* __restrict__ r, int* __restrict__ NN,
+                               const int* __restrict__ off, int* __restrict__ nbr, float* __restrict__ img) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_atoms) return;
+  const int n1 = atoms[k];
+  const int4 ac = acell[k];
+  const int4 gd = grid[ac.w];
+  const float* h = box + 18 * (size_t)grid_cfg[ac.w];
+  float hh[18];
+#pragma unroll
+  for (int q = 0; q < 18; ++q) hh[q] = h[q];
+  const float x1 = r[n1], y1 = r[n1 + N], z1 = r[n1 + 2 * (size_t)N];
+  int count = 0;
+  const int base = FILL ? off[n1] : 0;
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int cx = (ac.x + dx + gd.x) % gd.x, cy = (ac.y + dy + gd.y) % gd.y, cz = (ac.z + dz + gd.z) % gd.z;
+        const int cell = gd.w + (cz * gd.y + cy) * gd.x + cx;
+        for (int q = cell_start[cell]; q < cell_start[cell + 1]; ++q) {
+          const int n2 = cell_atoms[q];
+          if (n2 == n1) continue;
+          float ix, iy, iz;
+          if (pair_within<MODE>(hh, rc2, r, N, x1, y1, z1, n2, ix, iy, iz)) {
+            if (FILL) {
+              nbr[base + count] = n2;
+              img[3 * (size_t)(base + count) + 0] = ix;
+              img[3 * (size_t)(base + count) + 1] = iy;
+              img[3 * (size_t)(base + count) + 2] = iz;
+            }
+            ++count;
+          }
+        }
+      }
+  if constexpr (!FILL) {
+    NN[n1] = count;
+  } else {
+    // ascending neighbor index, as the reference's n2 loop produces them (insertion sort)
+    for (int a = base + 1; a < base + count; ++a) {
+      const int key = nbr[a];
+      const float kx = img[3 * (size_t)a], ky = img[3 * (size_t)a + 1], kz = img[3 * (size_t)a + 2];
+      int b = a - 1;
+      while (b >= base && nbr[b] > key) {
+        nbr[b + 1] = nbr[b];
+        img[3 * (size_t)(b + 1) + 0] = img[3 * (size_t)b + 0];
+        img[3 * (size_t)(b + 1) + 1] = img[3 * (size_t)b + 1];
+        img[3 * (size_t)(b + 1) + 2] = img[3 * (size_t)b + 2];
+        --b;
+      }
+      nbr[b + 1] = key;
+      img[3 * (size_t)(b + 1) + 0] = kx;
+      img[3 * (size_t)(b + 1) + 1] = ky;
+      img[3 * (size_t)(b + 1) + 2] = kz;
+    }
   }
 }
 
@@ -106,17 +185,14 @@ __global__ void neighbor_reference(int N, const int* __restrict__ Na, const int*
     int count = 0;
     for (int n2 = n_begin; n2 < n_end; ++n2) {
       if (n2 == n1) continue;
-      float x12 = __fsub_rn(r[n2], x1);
-      float y12 = __fsub_rn(r[n2 + N], y1);
-      float z12 = __fsub_rn(r[n2 + 2 * (size_t)N], z1);
       float ix, iy, iz;
-      mic32<MODE>(hh, x12, y12, z12, ix, iy, iz);
-      const float d2 = dot3<MODE>(x12, x12, y12, y12, z12, z12);
-      if (d2 < rc2) NL[(size_t)count++ * N + n1] = n2;
+      if (pair_within<MODE>(hh, rc2, r, N, x1, y1, z1, n2, ix, iy, iz)) NL[(size_t)count++ * N + n1] = n2;
     }
     NN[n1] = count;
   }
 }
+
+constexpr int kCellMinAtoms = 2048;  // automatic cell lists from this configuration size on
 
 constexpr double kRiAlpha = 0.2;                  // ri.cu:26
 constexpr double kRiPiFactor = 0.225675833419103;  // ri.cu:28, 2*alpha/sqrt(pi)
@@ -245,6 +321,85 @@ int neighbor_reference_layout(int Nc, int N, int max_Na, const int* Na, const in
   return GPUGA_OK;
 }
 
+// Cell lists of the configurations that take the O(N) path: every cell at least
+// rc (with a 1e-4 margin for the FP32 test) wide along each cell vector's
+// normal and at least 3 cells per direction, so that the 27 cells around an
+// atom hold every atom within rc exactly once under the nearest-image rule.
+struct CellLists {
+  std::vector<uint8_t> skip;        // per configuration: 1 = cell path
+  std::vector<int> atoms;           // atoms of cell-path configurations
+  std::vector<int4> acell;          // per listed atom: cell x, y, z and grid row
+  std::vector<int4> grid;           // per cell-path configuration: nx, ny, nz, first cell
+  std::vector<int> grid_cfg;        // configuration of each grid row
+  std::vector<int> cell_start;      // [cells + 1]
+  std::vector<int> cell_atoms;      // atoms by cell, ascending within a cell
+};
+
+void build_cell_lists(const Engine* e, CellLists* cl) {
+  const TrainingSet& ts = e->ts;
+  const int mode = e->opt.neighbor_cells;  // 0 auto, 1 wherever the grid allows, 2 never
+  const double rc = e->spec.cutoff * (1.0 + 1e-4);
+  cl->skip.assign(ts.Nc, 0);
+  cl->cell_start.assign(1, 0);
+  if (mode == 2) return;
+  for (int c = 0; c < ts.Nc; ++c) {
+    const int Na = ts.Na[c];
+    if (mode == 0 && Na < kCellMinAtoms) continue;
+    const float* h = &ts.h[18 * (size_t)c];
+    // cell vectors are the columns of h; width along a = V / |b x c|, etc.
+    const double a[3] = {h[0], h[3], h[6]}, b[3] = {h[1], h[4], h[7]}, cc[3] = {h[2], h[5], h[8]};
+    auto cross = [](const double* u, const double* v, double* w) {
+      w[0] = u[1] * v[2] - u[2] * v[1];
+      w[1] = u[2] * v[0] - u[0] * v[2];
+      w[2] = u[0] * v[1] - u[1] * v[0];
+    };
+    double bc[3], ca[3], ab[3];
+    cross(b, cc, bc);
+    cross(cc, a, ca);
+    cross(a, b, ab);
+    const double vol = std::fabs(a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2]);
+    const double wa = vol / std::sqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2]);
+    const double wb = vol / std::sqrt(ca[0] * ca[0] + ca[1] * ca[1] + ca[2] * ca[2]);
+    const double wc = vol / std::sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2]);
+    const int nx = (int)std::floor(wa / rc), ny = (int)std::floor(wb / rc), nz = (int)std::floor(wc / rc);
+    if (!(vol > 0) || nx < 3 || ny < 3 || nz < 3) continue;
+    if ((long long)nx * ny * nz > 4LL * Na + 64) continue;  // sparse grid: the scan is as cheap
+    cl->skip[c] = 1;
+    const int g = (int)cl->grid.size();
+    const int first = (int)cl->cell_start.size() - 1;
+    const int ncell = nx * ny * nz;
+    cl->grid.push_back(make_int4(nx, ny, nz, first));
+    cl->grid_cfg.push_back(c);
+    // fractional coordinates with the inverse of the FP32 box, in FP64
+    const double det = a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2];
+    std::vector<int> cell_of(Na), count(ncell, 0);
+    for (int k = 0; k < Na; ++k) {
+      const int i = ts.Na_sum[c] + k;
+      const double x = ts.r[i], y = ts.r[i + ts.N], z = ts.r[i + 2 * (size_t)ts.N];
+      // s = h^-1 r with h^-1 rows = (b x c, c x a, a x b) / det
+      double s[3] = {(bc[0] * x + bc[1] * y + bc[2] * z) / det, (ca[0] * x + ca[1] * y + ca[2] * z) / det,
+                     (ab[0] * x + ab[1] * y + ab[2] * z) / det};
+      const int n[3] = {nx, ny, nz};
+      int ci[3];
+      for (int q = 0; q < 3; ++q) {
+        s[q] -= std::floor(s[q]);
+        ci[q] = std::min(n[q] - 1, std::max(0, (int)(s[q] * n[q])));
+      }
+      cell_of[k] = (ci[2] * ny + ci[1]) * nx + ci[0];
+      ++count[cell_of[k]];
+      cl->atoms.push_back(i);
+      cl->acell.push_back(make_int4(ci[0], ci[1], ci[2], g));
+    }
+    std::vector<int> start(ncell + 1, 0);
+    for (int q = 0; q < ncell; ++q) start[q + 1] = start[q] + count[q];
+    const int base = (int)cl->cell_atoms.size();
+    cl->cell_atoms.resize(base + Na);
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (int k = 0; k < Na; ++k) cl->cell_atoms[base + fill[cell_of[k]]++] = ts.Na_sum[c] + k;
+    for (int q = 1; q <= ncell; ++q) cl->cell_start.push_back(base + start[q]);
+  }
+}
+
 int build_geometry(Engine* e) {
   DevSet& d = e->d;
   const TrainingSet& ts = e->ts;
@@ -254,9 +409,47 @@ int build_geometry(Engine* e) {
 
   GPUGA_TRY(e->alloc(&d.NN, N));
   GPUGA_TRY(e->alloc(&d.off, N + 1));
+  CellLists cl;
+  build_cell_lists(e, &cl);
+  uint8_t* d_skip = nullptr;
+  int *d_catoms = nullptr, *d_gcfg = nullptr, *d_cstart = nullptr, *d_cell_atoms = nullptr;
+  int4 *d_acell = nullptr, *d_grid = nullptr;
+  const int n_cell_atoms = (int)cl.atoms.size();
+  if (n_cell_atoms > 0) {
+    GPUGA_CUDA(cudaMalloc(&d_skip, Nc));
+    GPUGA_CUDA(cudaMalloc(&d_catoms, sizeof(int) * n_cell_atoms));
+    GPUGA_CUDA(cudaMalloc(&d_acell, sizeof(int4) * n_cell_atoms));
+    GPUGA_CUDA(cudaMalloc(&d_grid, sizeof(int4) * cl.grid.size()));
+    GPUGA_CUDA(cudaMalloc(&d_gcfg, sizeof(int) * cl.grid_cfg.size()));
+    GPUGA_CUDA(cudaMalloc(&d_cstart, sizeof(int) * cl.cell_start.size()));
+    GPUGA_CUDA(cudaMalloc(&d_cell_atoms, sizeof(int) * cl.cell_atoms.size()));
+    GPUGA_CUDA(cudaMemcpy(d_skip, cl.skip.data(), Nc, cudaMemcpyHostToDevice));
+    GPUGA_CUDA(cudaMemcpy(d_catoms, cl.atoms.data(), sizeof(int) * n_cell_atoms, cudaMemcpyHostToDevice));
+    GPUGA_CUDA(cudaMemcpy(d_acell, cl.acell.data(), sizeof(int4) * n_cell_atoms, cudaMemcpyHostToDevice));
+    GPUGA_CUDA(cudaMemcpy(d_grid, cl.grid.data(), sizeof(int4) * cl.grid.size(), cudaMemcpyHostToDevice));
+    GPUGA_CUDA(cudaMemcpy(d_gcfg, cl.grid_cfg.data(), sizeof(int) * cl.grid_cfg.size(), cudaMemcpyHostToDevice));
+    GPUGA_CUDA(cudaMemcpy(d_cstart, cl.cell_start.data(), sizeof(int) * cl.cell_start.size(), cudaMemcpyHostToDevice));
+    GPUGA_CUDA(cudaMemcpy(d_cell_atoms, cl.cell_atoms.data(), sizeof(int) * cl.cell_atoms.size(),
+                          cudaMemcpyHostToDevice));
+  }
+  auto free_cells = [&]() {
+    cudaFree(d_skip);
+    cudaFree(d_catoms);
+    cudaFree(d_acell);
+    cudaFree(d_grid);
+    cudaFree(d_gcfg);
+    cudaFree(d_cstart);
+    cudaFree(d_cell_atoms);
+  };
   neighbor_scan<kMicMode, false><<<Nc, 256, 0, st>>>(N, d.Na, d.Na_sum, rc2, d.h, d.r, d.NN, nullptr, nullptr,
-                                                    nullptr);
+                                                    nullptr, d_skip);
   GPUGA_CUDA(cudaGetLastError());
+  if (n_cell_atoms > 0) {
+    neighbor_cells<kMicMode, false><<<(n_cell_atoms + 127) / 128, 128, 0, st>>>(
+        N, n_cell_atoms, d_catoms, d_acell, d_grid, d_gcfg, d_cstart, d_cell_atoms, rc2, d.h, d.r, d.NN, nullptr,
+        nullptr, nullptr);
+    GPUGA_CUDA(cudaGetLastError());
+  }
   e->h_NN.assign(N, 0);
   GPUGA_CUDA(cudaMemcpyAsync(e->h_NN.data(), d.NN, sizeof(int) * N, cudaMemcpyDeviceToHost, st));
   GPUGA_CUDA(cudaStreamSynchronize(st));
@@ -281,8 +474,15 @@ int build_geometry(Engine* e) {
   float* img = nullptr;
   GPUGA_CUDA(cudaMalloc(&img, sizeof(float) * 3 * (size_t)std::max(B, 1)));
   GPUGA_TRY(e->alloc(&d.nbr, std::max(B, 1)));
-  neighbor_scan<kMicMode, true><<<Nc, 256, 0, st>>>(N, d.Na, d.Na_sum, rc2, d.h, d.r, d.NN, d.off, d.nbr, img);
+  neighbor_scan<kMicMode, true><<<Nc, 256, 0, st>>>(N, d.Na, d.Na_sum, rc2, d.h, d.r, d.NN, d.off, d.nbr, img,
+                                                   d_skip);
   GPUGA_CUDA(cudaGetLastError());
+  if (n_cell_atoms > 0) {
+    neighbor_cells<kMicMode, true><<<(n_cell_atoms + 127) / 128, 128, 0, st>>>(
+        N, n_cell_atoms, d_catoms, d_acell, d_grid, d_gcfg, d_cstart, d_cell_atoms, rc2, d.h, d.r, d.NN, d.off,
+        d.nbr, img);
+    GPUGA_CUDA(cudaGetLastError());
+  }
 
   // per-atom config index for the geometry kernel
   std::vector<int> atom_cfg(N);
@@ -315,6 +515,7 @@ int build_geometry(Engine* e) {
   GPUGA_CUDA(cudaStreamSynchronize(st));
   cudaFree(img);
   cudaFree(d_atom_cfg);
+  free_cells();
 
   e->h_nbr.assign(std::max(B, 1), 0);
   GPUGA_CUDA(cudaMemcpy(e->h_nbr.data(), d.nbr, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost));

@@ -15,11 +15,11 @@
 //   2^r = sum_{i<=7} (r ln 2)^i / i!  (Taylor series; truncation < 6e-9 relative).
 //
 // The series are the Taylor expansions of atanh and of exp; the double-float
-// steps are Dekker's exact product (via FMA) and Fast2Sum.  About 40
-// instructions, a third of a general-purpose powf, which also handles zero,
-// negative, subnormal and non-finite arguments: those go to powf itself here.
-// Results below about 2^-125 flush to zero and results above about 2^127
-// become +inf.
+// steps are Dekker's exact product (via FMA) and Fast2Sum.  Domain: x > 0
+// (the bond order only raises zeta >= 1e-16 and 1 + zeta^n); NaN x returns
+// NaN, x = +inf and |y log2 x| > 125 give +inf or 0 (results below 2^-125
+// flush to zero), zero and subnormal x give 0 for y > 0.  Negative x is not
+// accepted.
 #pragma once
 #include <cmath>
 #include <cstdint>
@@ -61,15 +61,8 @@ GPUGA_HD float pdd_rcp(float t) {
 #endif
 }
 
-#ifdef __CUDACC__
-__host__ __device__ __noinline__ inline float pdd_general(float x, float y) { return powf(x, y); }
-#else
-inline float pdd_general(float x, float y) { return powf(x, y); }
-#endif
-
 GPUGA_HD float powf_dd(float x, float y) {
-  // arguments outside the accepted domain go to the general-purpose powf
-  if (!(x >= 1.17549435e-38f && x < INFINITY && fabsf(y) < INFINITY)) return pdd_general(x, y);
+  if (x != x) return x;  // NaN
   // x = 2^e m with m in [sqrt(1/2), sqrt(2))
   const int32_t ix = pdd_as_int(x);
   const int32_t e = (ix - 0x3f3504f3) >> 23;
@@ -104,9 +97,7 @@ GPUGA_HD float powf_dd(float x, float y) {
   const float t_h = y * L_h;
   float t_l = fmaf(y, L_h, -t_h);
   t_l = fmaf(y, L_l, t_l);
-  if (t_h < -125.0f) return 0.0f;
-  if (t_h > 127.0f) return INFINITY;
-  // 2^t = 2^k 2^r
+  // 2^t = 2^k 2^r (out of range: selected away at the end, no branch)
   const float k = rintf(t_h);
   const float r = (t_h - k) + t_l;
   float u = fmaf(r, 1.5252733804059838e-05f, 1.5403530393381606e-04f);
@@ -116,7 +107,8 @@ GPUGA_HD float powf_dd(float x, float y) {
   u = fmaf(r, u, 2.402265069591007e-01f);
   u = fmaf(r, u, 6.931471805599453e-01f);
   const float p2 = fmaf(r, u, 1.0f);
-  return pdd_as_float(pdd_as_int(p2) + (int32_t)k * (1 << 23));
+  const float v = pdd_as_float(pdd_as_int(p2) + (int32_t)k * (1 << 23));
+  return fabsf(t_h) <= 125.0f ? v : (t_h > 0.0f ? INFINITY : 0.0f);
 }
 
 }  // namespace gpuga

@@ -162,6 +162,24 @@ def make(config: int, seed: int | None = None, Nc: int | None = None) -> dict:
     return data
 
 
+def diamond_set(reps_list, Nc_force: int, seed: int = 11, strain: float = 0.03, sigma: float = 0.1,
+                P: int = 64) -> dict:
+    """Minimal-Tersoff Si set of diamond supercells reps x reps x reps (8 reps^3 atoms each), with the
+    bounds and teacher draw of workload 2 -- e.g. a few configurations of thousands of atoms."""
+    rng = np.random.default_rng(seed)
+    configs = []
+    for n in reps_list:
+        frac, cell = _structure(DIAMOND, np.eye(3) * 5.43, (n, n, n))
+        configs.append(_config(rng, frac, cell, np.zeros(len(frac)), strain, sigma))
+    spec = dict(potential_type=1, num_neurons=0, cutoff=3.0, w_force=0.05, w_energy=0.15, w_stress=0.8,
+                pmin=SI_TERSOFF_BOUNDS[:, 0].copy(), pmax=SI_TERSOFF_BOUNDS[:, 1].copy(),
+                ga=dict(population_size=P, parent_number=P // 2, mutation_rate=0.2, maximum_generation=1000))
+    data = _assemble(configs, Nc_force, spec)
+    data["teacher01"] = rng.uniform(0, 1, size=9).astype(np.float32)
+    data["name"] = "diamond_set"
+    return data
+
+
 def teacher_params(data) -> np.ndarray:
     return _decode(data["pmin"], data["pmax"], data["teacher01"]).astype(np.float64)
 

@@ -49,6 +49,9 @@ typedef struct gpuga_options {
   float nn2b_r1;       /* NN2B taper start, reference default 7 (nn2b.cuh:36) */
   float nn2b_r2;       /* NN2B taper end, reference default 8 (nn2b.cuh:37) */
   int verbose;         /* print the reference's start-up banners */
+  int neighbor_cells;  /* neighbor build: 0 cell lists for configurations of >= 2048 atoms (default),
+                          1 cell lists wherever the box holds >= 3 cells of width rc per direction,
+                          2 the O(Na^2) scan of neighbor.cu:30-66 everywhere; the lists are identical */
 } gpuga_options;
 
 /* Fills *opt with the reference's semantics (batched path, graphs on, NN2B taper 7..8 A, force quirk kept). */

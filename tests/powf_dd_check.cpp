@@ -40,8 +40,10 @@ int main(int argc, char** argv) {
   bad += gpuga::powf_dd(2.0f, 3.0f) != 8.0f;
   bad += gpuga::powf_dd(4.0f, -0.5f) != 0.5f;
   bad += !(gpuga::powf_dd(0.0f, 2.0f) == 0.0f);
-  bad += !std::isnan(gpuga::powf_dd(-2.0f, 0.5f));
+  bad += !std::isnan(gpuga::powf_dd(NAN, 0.5f));
   bad += !(gpuga::powf_dd(INFINITY, 1.0f) == INFINITY);
+  bad += !(gpuga::powf_dd(INFINITY, -1.0f) == 0.0f);
+  bad += !(gpuga::powf_dd(3.0f, 200.0f) == INFINITY);
   bad += gpuga::powf_dd(1e-30f, 4.0f) != 0.0f;  // 1e-120 flushes to zero
   printf("%ld %.6f %.6f %d\n", cnt, mx, sum / cnt, bad);
   return 0;
