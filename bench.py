@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--plain-individuals", type=int, default=48)
     ap.add_argument("--configs", type=int, default=None, help="override the workload's configuration count")
     ap.add_argument("--population", type=int, default=None, help="override the workload's population size")
+    ap.add_argument("--neurons", type=int, default=None,
+                    help="NN2B hidden width of workload 4 (default 16; the reference arm needs <= 10)")
     ap.add_argument("--serving", action="store_true", help="serving benchmark (workload 5) instead")
     ap.add_argument("--serving-jobs", type=int, default=32)
     ap.add_argument("--serving-generations", type=int, default=20)
@@ -170,6 +172,21 @@ def ncu_traffic(kernel: str, workload: int, units: float):
     return None
 
 
+def ncu_inst_per_unit(kernel: str, workload: int):
+    """Warp instructions per (individual, atom) of `kernel` from the ncu capture summarised in
+    profiles/tersoff_batched_mid_ncu.md (lines `inst: workload=W kernel=K warp_inst_per_unit=X`)."""
+    try:
+        lines = open(os.path.join(ROOT, "profiles", "tersoff_batched_mid_ncu.md")).read().splitlines()
+    except OSError:
+        return None
+    for line in lines:
+        if line.startswith("inst:"):
+            kv = dict(tok.split("=", 1) for tok in line.split()[1:])
+            if int(kv["workload"]) == workload and kv["kernel"] == kernel:
+                return float(kv["warp_inst_per_unit"])
+    return None
+
+
 # ----------------------------------------------------------------------------- workload
 def oracle_evaluator():
     from oracle import oracle
@@ -195,10 +212,10 @@ def engine_opts(data, device):
     return kw
 
 
-def build_workload(workload: int, device: int, Nc=None, P=None):
+def build_workload(workload: int, device: int, Nc=None, P=None, neurons=None):
     """Synthetic set with teacher targets evaluated by the engine's own FP64 path."""
     from gpuga_b200 import Fitness, synth
-    data = synth.make(workload, Nc=Nc)
+    data = synth.make(workload, Nc=Nc, neurons=neurons)
     if P:
         data["ga"] = dict(data["ga"], population_size=P, parent_number=P // 2)
     with Fitness(arrays=data, **engine_opts(data, device)) as e0:
@@ -216,7 +233,7 @@ def run_ours(args, dist: Dist):
     dev = dist.local_rank
     torch.cuda.set_device(dev)
     L = _lib.load()
-    data, e = build_workload(args.workload, dev, args.configs, args.population)
+    data, e = build_workload(args.workload, dev, args.configs, args.population, args.neurons)
     P = int(data["ga"]["population_size"])
     d = e.number_of_variables
     Natoms = e.N
@@ -281,11 +298,23 @@ def run_ours(args, dist: Dist):
     dom = max(launches, key=lambda x: x["ms"])
     gen_flops = sum(x["flops"] for x in launches)
     traffic = ncu_traffic(dom["kernel"], args.workload, dom["units"])
+    # instruction-issue bound of the same launch: warp instructions (ncu count per unit) issued per
+    # second against 4 schedulers x SMs x SM clock
+    ipu = ncu_inst_per_unit(dom["kernel"], args.workload)
+    issue = None
+    if ipu and dom["ms"] > 0:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = (clock_info or {}).get("sm_mhz") or measured_peaks().get("sm_max_mhz") or 1965.0
+        achieved = ipu * dom["units"] / (dom["ms"] * 1e-3)
+        peak = 4.0 * sms * mhz * 1e6
+        issue = {"warp_inst_per_unit": ipu, "achieved_warp_inst_per_s": achieved, "peak_warp_inst_per_s": peak,
+                 "frac": achieved / peak, "source": "ncu smsp__inst_executed, profiles/tersoff_batched_mid_ncu.md"}
     roofline = {"bound": "fp32", "kernel": dom["kernel"], "achieved": dom["tflops"], "peak": peak_fp32.value,
                 "unit": "TFLOP/s", "frac": dom["tflops"] / peak_fp32.value if dom["tflops"] else None,
                 "traffic": traffic, "peak_source": "measured: FFMA-chain calibration kernel on this GPU",
                 "algorithmic": "FP32 flops of the batched formulation (FMA=2), transcendentals separate",
                 "ms_per_launch": dom["ms"], "launches": launches,
+                "issue": issue,
                 "generation": {"flops": gen_flops, "ms": ms_per_step,
                                "achieved": gen_flops / (ms_per_step * 1e-3) / 1e12,
                                "frac": gen_flops / (ms_per_step * 1e-3) / 1e12 / peak_fp32.value}}
@@ -407,11 +436,12 @@ def run_reference(args, dist: Dist):
     if not os.path.exists(probe):
         return {"impl": "reference", "unavailable": "oracle/_ref/ref_probe was not built (needs the reference sources)"}
     from gpuga_b200 import synth
-    data = synth.make(args.workload, Nc=args.configs)
+    data = synth.make(args.workload, Nc=args.configs, neurons=args.neurons)
     if args.population:
         data["ga"] = dict(data["ga"], population_size=args.population)
-    if args.workload == 4:
-        return {"impl": "reference", "unavailable": "the reference NN2B holds at most 10 neurons (nn2b.cuh:27-33)"}
+    if args.workload == 4 and int(data["num_neurons"]) > 10:
+        return {"impl": "reference", "unavailable": "the reference NN2B holds at most 10 neurons (nn2b.cuh:27-33); "
+                                                    "run with --neurons 10"}
     data = synth.fill_targets(data, oracle_evaluator())
     d = synth.write_dir(data, tempfile.mkdtemp(prefix="gpuga_ref_"))
     P = int(data["ga"]["population_size"])

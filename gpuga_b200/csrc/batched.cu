@@ -25,6 +25,8 @@
 #include <cmath>
 #include <tuple>
 
+#include <cuda_pipeline.h>
+
 #include "engine.hpp"
 #include "powf_dd.cuh"
 
@@ -35,9 +37,11 @@ namespace gpuga {
 // cr = D0/(S-1), ca = S*D0/(S-1), r0; then n, beta, h, R1, R2, pi/(R2-R1), -1/(2n).
 enum { TC_LR = 0, TC_LA = 2, TC_CR = 4, TC_CA = 6, TC_R0 = 8, TC_EN = 10, TC_BETA, TC_H, TC_R1, TC_R2, TC_PF,
        TC_MHON, TC_COUNT };
-// RI (ri.cu:36-110): qq[3], a[3], b[3] = 1/rho, c[3], rc, v_rc, dv_rc, Morse lr, la, cr, ca, r0.
+// RI (ri.cu:36-110): qq[3], a[3], b[3] = 1/rho, c[3], rc, v_rc, dv_rc, Morse lr, la, cr, ca, r0,
+// then the FP64 remainders of b[3], lr and la (their FP32 roundings would otherwise shift the
+// exponents |d/rho|, |lr (d - r0)| of up to ~20 by 2^-24 relative).
 enum { RC_QQ = 0, RC_A = 3, RC_B = 6, RC_C = 9, RC_RC = 12, RC_VRC, RC_DVRC, RC_LR, RC_LA, RC_CR, RC_CA, RC_R0,
-       RC_COUNT };
+       RC_BLO, RC_LRLO = RC_BLO + 3, RC_LALO, RC_COUNT };
 
 int consts_per_individual(const DevSet& d) {
   if (d.potential_type == 1 || d.potential_type == 2) return TC_COUNT;
@@ -65,6 +69,7 @@ __global__ void decode_jobs(const JobView* __restrict__ jobs, const int2* __rest
   const float* x = J.pop + (size_t)p * nv;
   auto par = [&](int m) { return (double)decode1(pmin[m], pmax[m], x[m]); };
   auto put = [&](int k, double v) { consts[(size_t)k * Pstride + p] = (float)v; };
+  auto put_lo = [&](int k, double v) { consts[(size_t)k * Pstride + p] = (float)(v - (double)(float)v); };
   if (potential_type == 1 || potential_type == 2) {
     const int off = num_types == 2 ? 4 : 0;
     for (int s = 0; s < 2; ++s) {
@@ -93,6 +98,7 @@ __global__ void decode_jobs(const JobView* __restrict__ jobs, const int2* __rest
     for (int t = 0; t < 3; ++t) {
       put(RC_A + t, par(1 + 3 * t));
       put(RC_B + t, 1.0 / par(2 + 3 * t));
+      put_lo(RC_BLO + t, 1.0 / par(2 + 3 * t));
       put(RC_C + t, par(3 + 3 * t));
     }
     const double rc = par(10), alpha = 0.2, pif = 0.225675833419103;
@@ -104,6 +110,8 @@ __global__ void decode_jobs(const JobView* __restrict__ jobs, const int2* __rest
     const double d0 = par(11), al = par(12), r0 = par(13), s = par(14);
     put(RC_LR, sqrt(2.0 * s) * al);
     put(RC_LA, sqrt(2.0 / s) * al);
+    put_lo(RC_LRLO, sqrt(2.0 * s) * al);
+    put_lo(RC_LALO, sqrt(2.0 / s) * al);
     put(RC_CR, d0 / (s - 1.0));
     put(RC_CA, s * d0 / (s - 1.0));
     put(RC_R0, r0);
@@ -465,10 +473,15 @@ __global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_ba
 
 // --------------------------------------------------------------------------- RI / NN2B
 // RI pair term (ri.cu:77-110) with the geometry-only Coulomb pieces precomputed:
-// gri = (1/d, 1/d^6, erfc(alpha d)/d, erfc(alpha d)/d^2 + 2 alpha/sqrt(pi) exp(-alpha^2 d^2)/d).
+// gri = (d - (float)d, 1/d^6, erfc(alpha d)/d, erfc(alpha d)/d^2 + 2 alpha/sqrt(pi) exp(-alpha^2 d^2)/d).
 // Returns U(d) in p2 and dU/dd in fd.
+//
+// The exponents d/rho (Buckingham) and lr (d - r0), la (d - r0) (Morse) reach
+// ~20, so their FP32 rounding alone would move exp() by ~1e-6 relative; they
+// are formed as hi + lo (exact FMA residuals, the FP64 remainders of d, 1/rho,
+// lr and la) and exp(-(hi + lo)) = exp(-hi) (1 - lo).
 struct RIC {  // the lane's RI constants, loaded once per work item
-  float qq[3], a[3], b[3], c6[3], c[3], rc, vrc, dvrc, lr, la, cr, ca, r0;
+  float qq[3], a[3], b[3], blo[3], c6[3], c[3], rc, vrc, dvrc, lr, la, lrlo, lalo, cr, ca, r0;
 };
 
 __device__ __forceinline__ void load_ri(const Consts& k, RIC& R) {
@@ -477,6 +490,7 @@ __device__ __forceinline__ void load_ri(const Consts& k, RIC& R) {
     R.qq[t] = k[RC_QQ + t];
     R.a[t] = k[RC_A + t];
     R.b[t] = k[RC_B + t];
+    R.blo[t] = k[RC_BLO + t];
     R.c[t] = k[RC_C + t];
     R.c6[t] = 6.0f * R.c[t];
   }
@@ -485,24 +499,39 @@ __device__ __forceinline__ void load_ri(const Consts& k, RIC& R) {
   R.dvrc = k[RC_DVRC];
   R.lr = k[RC_LR];
   R.la = k[RC_LA];
+  R.lrlo = k[RC_LRLO];
+  R.lalo = k[RC_LALO];
   R.cr = k[RC_CR];
   R.ca = k[RC_CA];
   R.r0 = k[RC_R0];
 }
 
+// exp(-x y) for x = xh + xl, y = yh + yl (double-float), to ~1 ulp of exp
+__device__ __forceinline__ float exp_neg_dd(float xh, float xl, float yh, float yl) {
+  const float p = xh * yh;
+  const float lo = fmaf(xh, yh, -p) + fmaf(xh, yl, xl * yh);
+  const float e = expf(-p);
+  return fmaf(-lo, e, e);
+}
+
 __device__ __forceinline__ void ri_pair(const RIC& R, int t, float d, float4 w, float& p2, float& fd) {
   const float a = t == 0 ? R.a[0] : (t == 1 ? R.a[1] : R.a[2]);
   const float b = t == 0 ? R.b[0] : (t == 1 ? R.b[1] : R.b[2]);
+  const float blo = t == 0 ? R.blo[0] : (t == 1 ? R.blo[1] : R.blo[2]);
   const float c = t == 0 ? R.c[0] : (t == 1 ? R.c[1] : R.c[2]);
   const float c6 = t == 0 ? R.c6[0] : (t == 1 ? R.c6[1] : R.c6[2]);
   const float qq = t == 0 ? R.qq[0] : (t == 1 ? R.qq[1] : R.qq[2]);
-  const float ex = expf(-d * b);
+  const float dlo = w.x;
+  const float ex = exp_neg_dd(d, dlo, b, blo);
   p2 = a * ex - c * w.y + qq * (w.z - R.vrc - R.dvrc * (d - R.rc));
-  fd = c6 * w.y * w.x - a * ex * b - qq * (w.w + R.dvrc);
+  fd = __fdividef(c6 * w.y, d) - a * ex * b - qq * (w.w + R.dvrc);
   if (t == 1) {
-    const float dr = d - R.r0;
-    const float fr = R.cr * expf(-R.lr * dr);
-    const float fa = R.ca * expf(-R.la * dr);
+    // d - r0 as hi + lo (TwoSum), then the two Morse exponentials
+    const float drh = d - R.r0;
+    const float bb = drh - d;
+    const float drl = ((d - (drh - bb)) + (-R.r0 - bb)) + dlo;
+    const float fr = R.cr * exp_neg_dd(drh, drl, R.lr, R.lrlo);
+    const float fa = R.ca * exp_neg_dd(drh, drl, R.la, R.lalo);
     p2 += fr - fa;
     fd += -R.lr * fr + R.la * fa;
   }
@@ -511,6 +540,10 @@ __device__ __forceinline__ void ri_pair(const RIC& R, int t, float d, float4 w, 
 // Compensated FP32 sum (Kahan): the running error c is subtracted from each
 // new term; value() is the sum in FP64.  Error about 2 eps sum|x| for any
 // order of terms, against (n - 1) eps sum|x| for a plain FP32 sum.
+// bonds per chunk of the RI pair pipeline (one bond per lane); two stages per warp
+constexpr int kPairChunk = 32;
+constexpr size_t kPairStageBytes = (size_t)kWarps * 2 * 2 * kPairChunk * sizeof(float4);
+
 struct KSum {
   float s = 0.f, c = 0.f;
   __device__ __forceinline__ void add(float x) {
@@ -649,41 +682,111 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
   double acc[kResK];
 #pragma unroll
   for (int k = 0; k < kResK; ++k) acc[k] = 0.0;
-  for (int il = warp; il < Na; il += kWarps) {
-    const int i = atom0 + il;
-    const int bbeg = FORCE ? S.off[i] : S.half_off[i];
-    const int bend = S.off[i + 1];
-    // per-atom sums over the atom's pairs: compensated FP32 (Kahan), added to the
-    // FP64 accumulators once per atom -- a per-pair FP64 add would cost two
-    // FP32->FP64 conversions per term, which run at a fraction of the FP32 rate
-    KSum ks[FORCE ? 3 : 7];
-    auto consume = [&](const float4& q, float p2, float fd) {
-      if (FORCE) {
-        ks[0].add(fd * q.x);
-        ks[1].add(fd * q.y);
-        ks[2].add(fd * q.z);
-      } else {
-        // unordered pair: full U and -r (x) r f2 with f2 = fd / d, i.e. -d fd u (x) u
-        ks[0].add(p2);
-        const float s = -q.w * fd;
-        const float sx = s * q.x, sy = s * q.y, sz = s * q.z;
-        ks[1].add(sx * q.x);
-        ks[2].add(sy * q.y);
-        ks[3].add(sz * q.z);
-        ks[4].add(sx * q.y);
-        ks[5].add(sy * q.z);
-        ks[6].add(sz * q.x);
-      }
-    };
-    if constexpr (KIND == 1) {
-#pragma unroll 2
-      for (int b = bbeg; b < bend; ++b) {
-        const float4 q = __ldg(&S.g32[b]);
-        float p2, fd;
-        ri_pair(R, S.ptype[b], q.w, __ldg(&S.gri[b]), p2, fd);
-        consume(q, p2, fd);
+  // per-atom sums over the atom's pairs: compensated FP32 (Kahan), added to the
+  // FP64 accumulators once per atom -- a per-pair FP64 add would cost two
+  // FP32->FP64 conversions per term, which run at a fraction of the FP32 rate
+  constexpr int NK = FORCE ? 3 : 7;
+  auto consume = [&](KSum* ks, const float4& q, float p2, float fd) {
+    if (FORCE) {
+      ks[0].add(fd * q.x);
+      ks[1].add(fd * q.y);
+      ks[2].add(fd * q.z);
+    } else {
+      // unordered pair: full U and -r (x) r f2 with f2 = fd / d, i.e. -d fd u (x) u
+      ks[0].add(p2);
+      const float s = -q.w * fd;
+      const float sx = s * q.x, sy = s * q.y, sz = s * q.z;
+      ks[1].add(sx * q.x);
+      ks[2].add(sy * q.y);
+      ks[3].add(sz * q.z);
+      ks[4].add(sx * q.y);
+      ks[5].add(sy * q.z);
+      ks[6].add(sz * q.x);
+    }
+  };
+  auto finish_atom = [&](int il, KSum* ks) {
+    if (FORCE) {
+      const int i = atom0 + il;
+      const double dx = ks[0].value() - (double)S.force_ref[i];
+      const double dy = ks[1].value() - (double)S.force_ref[i + N];
+      const double dz = ks[2].value() - (double)S.force_ref[i + 2 * (size_t)N];
+      acc[7] += dx * dx + dy * dy + dz * dz;
+      if (fdump && p < P) {
+        const int Nf = S.N_force;
+        fdump[((size_t)p * 3 + 0) * Nf + i] = (float)ks[0].value();
+        fdump[((size_t)p * 3 + 1) * Nf + i] = (float)ks[1].value();
+        fdump[((size_t)p * 3 + 2) * Nf + i] = (float)ks[2].value();
       }
     } else {
+#pragma unroll
+      for (int k = 0; k < 7; ++k) acc[k] += ks[k].value();
+    }
+#pragma unroll
+    for (int k = 0; k < NK; ++k) ks[k] = KSum{};
+  };
+  auto bond_range = [&](int il, int& bb, int& be) {
+    const int i = atom0 + il;
+    bb = FORCE ? S.off[i] : S.half_off[i];
+    be = S.off[i + 1];
+  };
+  KSum ks[NK];
+  if constexpr (KIND == 1) {
+    // The warp's pairs (atoms warp, warp + 8, ... and each atom's bonds) stream through a
+    // two-stage shared-memory buffer of kPairChunk bonds: while the warp evaluates one chunk,
+    // asynchronous copies (cp.async, 16 B per lane) bring the next one, so the L2 latency of the
+    // per-bond geometry is hidden behind the pair arithmetic.  Every atom yields at least one
+    // chunk (possibly empty: force items still owe the atom's force error).
+    float4* buf = reinterpret_cast<float4*>(smem + (size_t)kWarps * 32 * kResK * sizeof(double)) +
+                  (size_t)warp * 4 * kPairChunk;  // [stage][geometry | Coulomb terms][kPairChunk]
+    int f_il = warp, f_b = 0, f_e = 0;
+    if (f_il < Na) bond_range(f_il, f_b, f_e);
+    int q_il[2], q_b[2], q_n[2], q_pt[2];
+    bool q_last[2], q_has[2];
+    auto fetch = [&](int st) {
+      q_has[st] = f_il < Na;
+      if (!q_has[st]) return;
+      q_il[st] = f_il;
+      q_b[st] = f_b;
+      q_n[st] = min(kPairChunk, f_e - f_b);
+      f_b += q_n[st];
+      q_last[st] = f_b >= f_e;
+      if (q_last[st]) {
+        f_il += kWarps;
+        if (f_il < Na) bond_range(f_il, f_b, f_e);
+      }
+      if (lane < q_n[st]) {
+        const int bnd = q_b[st] + lane;
+        __pipeline_memcpy_async(buf + (2 * st) * kPairChunk + lane, S.g32 + bnd, sizeof(float4));
+        __pipeline_memcpy_async(buf + (2 * st + 1) * kPairChunk + lane, S.gri + bnd, sizeof(float4));
+        q_pt[st] = S.ptype[bnd];
+      }
+    };
+    fetch(0);
+    __pipeline_commit();
+    fetch(1);
+    __pipeline_commit();
+    for (int st = 0; q_has[st]; st ^= 1) {
+      __pipeline_wait_prior(1);  // the older of the two groups in flight (stage st) has landed
+      __syncwarp();
+      const float4* g = buf + (2 * st) * kPairChunk;
+      const float4* w = g + kPairChunk;
+      const int n = q_n[st], pt = q_pt[st];
+#pragma unroll 2
+      for (int k = 0; k < n; ++k) {
+        const float4 q = g[k];
+        float p2, fd;
+        ri_pair(R, __shfl_sync(0xffffffffu, pt, k), q.w, w[k], p2, fd);
+        consume(ks, q, p2, fd);
+      }
+      if (q_last[st]) finish_atom(q_il[st], ks);
+      __syncwarp();  // every lane is done with stage st before it is refilled
+      fetch(st);
+      __pipeline_commit();
+    }
+  } else {
+    for (int il = warp; il < Na; il += kWarps) {
+      int bbeg, bend;
+      bond_range(il, bbeg, bend);
       // two pairs per weight load up to 16 neurons (registers allow it), one above
       constexpr int NP = NMAX <= 16 ? 2 : 1;
       for (int b = bbeg; b < bend; b += NP) {
@@ -708,25 +811,11 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
               pu *= fc;
               fd = f2raw[u] * fc + pu * fcp;
             }
-            consume(q[u], pu, fd);
+            consume(ks, q[u], pu, fd);
           }
         }
       }
-    }
-    if (FORCE) {
-      const double dx = ks[0].value() - (double)S.force_ref[i];
-      const double dy = ks[1].value() - (double)S.force_ref[i + N];
-      const double dz = ks[2].value() - (double)S.force_ref[i + 2 * (size_t)N];
-      acc[7] += dx * dx + dy * dy + dz * dz;
-      if (fdump && p < P) {
-        const int Nf = S.N_force;
-        fdump[((size_t)p * 3 + 0) * Nf + i] = (float)ks[0].value();
-        fdump[((size_t)p * 3 + 1) * Nf + i] = (float)ks[1].value();
-        fdump[((size_t)p * 3 + 2) * Nf + i] = (float)ks[2].value();
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < 7; ++k) acc[k] += ks[k].value();
+      finish_atom(il, ks);
     }
   }
   reduce_item(it, P, S.Nc, acc, smem, res);
@@ -965,6 +1054,8 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
       }
     } else if (kind == 2) {
       smem += (size_t)32 * (nmax * nmax + 4 * nmax + 1) * sizeof(float);  // NNSmem<nmax>::floats
+    } else {
+      smem += kPairStageBytes;  // RI: the warps' two-stage pair buffers
     }
     const LaunchKey key{kind, zc, nmax, force ? 1 : 0};
     smem_need[key] = std::max(smem_need[key], smem);

@@ -7,7 +7,8 @@
 //   bonds    nbr[B], rev[B] (reverse bond), rev_sm[B] (the reverse bond's slot * Na + atom,
 //            local to the configuration), ptype[B] (pair set / RI pair type),
 //            g32[B] float4 (unit vector, d), g64[B] double4 (x,y,z,d),
-//            gri[B] float4 (RI geometry-only terms), image shift from the FP32 MIC
+//            gri[B] float4 (RI: FP64 remainder of d, and the geometry-only terms 1/d^6 and the
+//            damped Coulomb energy / force pieces)
 //   targets  force_ref[3N], E_ref[Nc], W_ref[6Nc] (FP64 copies of the FP32 inputs)
 //
 // Bond vectors use the periodic image chosen by the reference's FP32 rule and

@@ -230,10 +230,10 @@ __global__ void bond_geometry(int N, const int* __restrict__ atom_cfg, const flo
         const double v_rc = erfc(kRiAlpha * rc_fixed) / rc_fixed;
         const double dv_rc = -erfc(kRiAlpha * rc_fixed) / (rc_fixed * rc_fixed) -
                              kRiPiFactor * exp(-kRiAlpha * kRiAlpha * rc_fixed * rc_fixed) / rc_fixed;
-        gri[b] = make_float4((float)dinv, (float)(dinv3 * dinv3), (float)(e1 - v_rc - dv_rc * (d - rc_fixed)),
-                             (float)(e2 + dv_rc));
+        gri[b] = make_float4((float)(d - (double)(float)d), (float)(dinv3 * dinv3),
+                             (float)(e1 - v_rc - dv_rc * (d - rc_fixed)), (float)(e2 + dv_rc));
       } else {
-        gri[b] = make_float4((float)dinv, (float)(dinv3 * dinv3), (float)e1, (float)e2);
+        gri[b] = make_float4((float)(d - (double)(float)d), (float)(dinv3 * dinv3), (float)e1, (float)e2);
       }
     }
     int rb = off[j];  // minimal_tersoff.cu:368: slot 0 when the reverse is absent

@@ -88,8 +88,9 @@ def _assemble(configs, Nc_force, spec):
     return d
 
 
-def make(config: int, seed: int | None = None, Nc: int | None = None) -> dict:
-    """Geometry, bounds, weights, GA sizes and the teacher for one workload (targets still zero)."""
+def make(config: int, seed: int | None = None, Nc: int | None = None, neurons: int | None = None) -> dict:
+    """Geometry, bounds, weights, GA sizes and the teacher for one workload (targets still zero).
+    `neurons` sets the NN2B hidden width of workload 4 (16 by default; the reference holds at most 10)."""
     seed = config if seed is None else seed
     rng = np.random.default_rng(seed)
     a_si = 5.43
@@ -140,7 +141,7 @@ def make(config: int, seed: int | None = None, Nc: int | None = None) -> dict:
         teacher = rng.uniform(0, 1, size=15).astype(np.float32)
     elif config == 4:
         Nc = Nc or 200
-        n = 16
+        n = neurons or 16
         nv = n * (n + 4) + 1
         lat = np.eye(3) * a_si
         configs = []
