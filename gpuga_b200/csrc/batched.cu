@@ -582,9 +582,10 @@ struct NNSmem {
 // NP pairs of the same lane at once: every weight loaded from shared memory
 // feeds the NP pairs (the hidden-to-hidden loads, not the FMAs, bound a
 // single pair).  Each pair's arithmetic is the same sequence as for NP = 1.
-template <int NMAX, int NP>
+template <int NMAX, int NP, bool FULL>
 __device__ __forceinline__ void nn_pairs(const float* __restrict__ wsm, int lane, int n, const float (&d)[NP],
                                          float (&p2)[NP], float (&f2)[NP]) {
+  if (FULL) n = NMAX;  // every row present: the row loop unrolls completely
   constexpr int Q = NMAX / 4;
   const float4* W1 = reinterpret_cast<const float4*>(wsm);
   const float4* V = W1 + NMAX * Q * 32;
@@ -606,6 +607,7 @@ __device__ __forceinline__ void nn_pairs(const float* __restrict__ wsm, int lane
 #pragma unroll
   for (int u = 0; u < NP; ++u) p2[u] = f2[u] = 0.f;
   const int qa_end = (n + 3) >> 2;
+#pragma unroll (FULL ? NMAX / 4 : 1)
   for (int qa = 0; qa < qa_end; ++qa) {
     const float4 b1 = V[(2 * Q + qa) * 32 + lane];
     const float4 w2 = V[(3 * Q + qa) * 32 + lane];
@@ -797,7 +799,10 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
           q[u] = __ldg(&S.g32[min(b + u, bend - 1)]);
           d[u] = q[u].w;
         }
-        nn_pairs<NMAX, NP>(wsm, lane, nn, d, p2, f2raw);
+        if (nn == NMAX)
+          nn_pairs<NMAX, NP, true>(wsm, lane, nn, d, p2, f2raw);
+        else
+          nn_pairs<NMAX, NP, false>(wsm, lane, nn, d, p2, f2raw);
 #pragma unroll
         for (int u = 0; u < NP; ++u) {
           if (b + u < bend) {

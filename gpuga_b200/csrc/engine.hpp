@@ -241,14 +241,30 @@ int plain_find_force64(Engine* e, const double* params, double* F, double* W, do
 int plain_find_force32(Engine* e, const float* params, float* F, float* W, float* pe);
 
 // ga_device.cu: device-resident GA loop (selection, crossover, mutation on the GPU
-// from host-drawn plans); `sink` receives the ga.out lines of each finished window.
+// from host-drawn plans) for one GA or a batch of jobs sharing the launches.
 struct GA;
 struct DeviceGA;
+struct GABatch;
+// One GA: `generations` generations in windows; `sink` receives the ga.out lines of each window.
 int device_ga_advance(Engine* e, GA* ga, DeviceGA** state, int generations, int window,
                       const std::function<void(const std::string&)>& sink);
 void device_ga_free(DeviceGA* s);
 // The GA's stable ascending order of FP32-rounded fitness values on the device: order[r] = i.
 int device_rank(int device, int P, const double* fitness, int* order, float* sorted);
+// Batches: per-job state (two plan stages of `window` generations), then one batch of jobs whose
+// fitness comes from `ls` (job k of the launch set = job k of the batch).
+int device_ga_setup(const GA& ga, int window, DeviceGA** out);
+float* device_ga_population(DeviceGA* s);
+double* device_ga_fitness64(DeviceGA* s);
+const float* device_ga_history(const DeviceGA* s, int b);  // [n][1 + d] after ga_batch_wait
+void device_ga_draw(GA& ga, DeviceGA* s, int b, int g0, int n);
+int device_ga_upload(DeviceGA* s, int b, int n, cudaStream_t st);
+int device_ga_sync_host(GA* ga, DeviceGA* s, int generations, cudaStream_t st);
+int ga_batch_build(const std::vector<DeviceGA*>& jobs, LaunchSet* ls, GABatch** out);
+void ga_batch_free(GABatch* b);
+int ga_batch_window(GABatch* B, int b, int n, bool use_graph, bool timed, cudaStream_t st);
+int ga_batch_wait(GABatch* B, int b);
+int ga_batch_generation_ms(GABatch* B, int n, std::vector<double>* ms);
 
 // engine.cu
 int engine_create(const PotentialSpec& spec, TrainingSet&& ts, const gpuga_options& opt, Engine** out);

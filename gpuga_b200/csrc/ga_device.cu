@@ -1,22 +1,25 @@
 // Device-resident GA loop: the generation of ga.cu:73-212 with its selection,
-// crossover and mutation on the GPU, behind the batched fitness launches.
+// crossover and mutation on the GPU, behind the batched fitness launches, for
+// one GA or for every job of the serving loop at once.
 //
 // The random draws of a generation never depend on fitness values (parents are
 // chosen by rank from fixed cumulative probabilities, ga.cu:41-46, 200-212), so
-// the host draws them from the GA's own std::mt19937 stream, in the
-// reference's order, a window of generations ahead (GA::draw_plan), while the
-// device runs the previous window.  Per generation the device then runs, with
-// no host round trip:
+// the host draws them from each GA's own std::mt19937 stream, in the
+// reference's order, a window of generations ahead (GA::draw_plan).  Per
+// generation the device then runs, with no host round trip:
 //
-//   batched fitness  ->  ga_rank  ->  ga_breed  ->  ga_mutate  ->  ga_advance
+//   batched fitness (all jobs) -> ga_rank -> ga_breed -> ga_mutate -> ga_advance
 //
+// The four GA kernels cover all jobs of a batch in one launch each: a job
+// table holds every job's buffers and each block finds its job through a
+// block -> job map, as the fitness launches do with their work items.
 // ga_rank reproduces the reference's stable insertion sort (ga.cu:105-119)
 // exactly, NaN included: a NaN never moves and no value passes one, so the
 // sort is a stable sort of every NaN-free run between NaNs; each individual's
 // position is its segment start + the number of smaller values in its segment
 // + the number of equal values before it.  One generation is captured in a CUDA
-// graph (one per plan buffer) and replayed for every generation of a window;
-// a device counter tells the kernels which generation of the window they run.
+// graph per plan buffer and replayed for every generation of a window; per-job
+// device counters tell the kernels which generation of the window they run.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,14 +33,33 @@ namespace gpuga {
 
 // Largest population whose FP32 fitness vector fits the rank kernel's shared memory.
 constexpr int kMaxDevicePopulation = 49152;
+constexpr int kGABlock = 256;
 
-__global__ void ga_rank(int P, int d, const double* __restrict__ fit64, const float* __restrict__ pop,
-                        float* __restrict__ sorted, float* __restrict__ fit_sorted, float* __restrict__ hist,
-                        const int* __restrict__ gen, int* __restrict__ order) {
-  extern __shared__ float f[];
+// One row of a batch's GA job table (plan buffers of one stage).
+struct GAJob {
+  int P, d, parent_number, pairs_per_gen;
+  int rank_block0, breed_block0, mut_block0;
+  float* pop;           // [P][d]: evaluated, then overwritten by the next generation
+  float* sorted;        // [P][d]
+  float* fit32;         // [P] sorted FP32 fitness
+  const double* fit64;  // [P] from the fitness fold
+  float* hist;          // [window][1 + d]: best fitness and elite genes per generation
+  int* gen;             // generation within the window
+  const int* pairs;     // [window][pairs_per_gen][3]
+  const int* off;       // [window + 1] mutation offsets
+  const int* midx;
+  const float* mval;
+};
+
+// Ranks the FP32-rounded fitness values of one job (or of an explicit fitness
+// vector, for gpuga_ga_rank_device) and writes the sorted population, the
+// sorted fitness and the elite of the generation.
+__device__ __forceinline__ void rank_block(int P, int d, const double* __restrict__ fit64,
+                                           const float* __restrict__ pop, float* __restrict__ sorted,
+                                           float* __restrict__ fit_sorted, float* __restrict__ hist, int gen,
+                                           int* __restrict__ order, int i, float* f) {
   for (int j = threadIdx.x; j < P; j += blockDim.x) f[j] = __double2float_rn(fit64[j]);  // the GA ranks FP32 values
   __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
   const float fi = f[i];
   int r = i;
@@ -59,52 +81,93 @@ __global__ void ga_rank(int P, int d, const double* __restrict__ fit64, const fl
   float* dst = sorted + (size_t)r * d;
   for (int m = 0; m < d; ++m) dst[m] = src[m];
   if (r == 0) {
-    float* h = hist + (size_t)(*gen) * (d + 1);
+    float* h = hist + (size_t)gen * (d + 1);
     h[0] = fi;
     for (int m = 0; m < d; ++m) h[1 + m] = src[m];
   }
 }
 
+__global__ void ga_rank_jobs(const GAJob* __restrict__ jobs, const int* __restrict__ block_job) {
+  extern __shared__ float f[];
+  const GAJob& J = jobs[block_job[blockIdx.x]];
+  const int i = (blockIdx.x - J.rank_block0) * blockDim.x + threadIdx.x;
+  rank_block(J.P, J.d, J.fit64, J.pop, J.sorted, J.fit32, J.hist, *J.gen, nullptr, i, f);
+}
+
+__global__ void ga_rank_values(int P, const double* __restrict__ fit64, float* __restrict__ fit_sorted,
+                               int* __restrict__ order) {
+  extern __shared__ float f[];
+  rank_block(P, 0, fit64, nullptr, nullptr, fit_sorted, nullptr, 0, order, blockIdx.x * blockDim.x + threadIdx.x,
+             f);
+}
+
 // ga.cu:161-186 on the sorted population: rows below parent_number are the
 // parents, each pair of children takes genes [0, point) from one parent and
 // [point, d) from the other.
-__global__ void ga_breed(int P, int d, int parent_number, const int* __restrict__ pairs, int pairs_per_gen,
-                         const float* __restrict__ sorted, float* __restrict__ pop, const int* __restrict__ gen) {
-  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void ga_breed_jobs(const GAJob* __restrict__ jobs, const int* __restrict__ block_job) {
+  const GAJob& J = jobs[block_job[blockIdx.x]];
+  const int P = J.P, d = J.d;
+  const long long n = (long long)(blockIdx.x - J.breed_block0) * blockDim.x + threadIdx.x;
   if (n >= (long long)P * d) return;
   const int r = (int)(n / d), c = (int)(n - (long long)r * d);
   float v;
-  if (r < parent_number) {
-    v = sorted[n];
+  if (r < J.parent_number) {
+    v = J.sorted[n];
   } else {
-    const int m = r - parent_number;
-    const int* q = pairs + ((size_t)(*gen) * pairs_per_gen + m / 2) * 3;
+    const int m = r - J.parent_number;
+    const int* q = J.pairs + ((size_t)(*J.gen) * J.pairs_per_gen + m / 2) * 3;
     const int first = c < q[2] ? q[0] : q[1];
     const int second = c < q[2] ? q[1] : q[0];
-    v = sorted[(size_t)((m & 1) ? second : first) * d + c];
+    v = J.sorted[(size_t)((m & 1) ? second : first) * d + c];
   }
-  pop[n] = v;
+  J.pop[n] = v;
 }
 
 // ga.cu:188-198 with repeated genes already folded on the host.
-__global__ void ga_mutate(const int* __restrict__ off, const int* __restrict__ idx, const float* __restrict__ val,
-                          float* __restrict__ pop, const int* __restrict__ gen) {
-  const int g = *gen;
-  const int k = off[g] + blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < off[g + 1]) pop[idx[k]] = val[k];
+__global__ void ga_mutate_jobs(const GAJob* __restrict__ jobs, const int* __restrict__ block_job) {
+  const GAJob& J = jobs[block_job[blockIdx.x]];
+  const int g = *J.gen;
+  const int k = J.off[g] + (blockIdx.x - J.mut_block0) * blockDim.x + threadIdx.x;
+  if (k < J.off[g + 1]) J.pop[J.midx[k]] = J.mval[k];
 }
 
-__global__ void ga_advance(int* gen) { *gen += 1; }
+__global__ void ga_advance_jobs(const GAJob* __restrict__ jobs, int njobs) {
+  for (int j = threadIdx.x; j < njobs; j += blockDim.x) *jobs[j].gen += 1;
+}
 
+// The GA kernels of several jobs, launched together behind one launch set.
+struct GABatch {
+  std::vector<DeviceGA*> jobs;
+  LaunchSet* ls = nullptr;
+  GAJob* d_table[2] = {nullptr, nullptr};
+  int *d_rank_map = nullptr, *d_breed_map = nullptr, *d_mut_map = nullptr;
+  int n_rank = 0, n_breed = 0, n_mut = 0;
+  size_t rank_smem = 0;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  std::vector<cudaEvent_t> gen_ev;  // per-generation timing events of the last window
+  ~GABatch() {
+    for (int b = 0; b < 2; ++b) {
+      if (graph[b]) cudaGraphExecDestroy(graph[b]);
+      if (done[b]) cudaEventDestroy(done[b]);
+      cudaFree(d_table[b]);
+    }
+    for (cudaEvent_t e : gen_ev) cudaEventDestroy(e);
+    cudaFree(d_rank_map);
+    cudaFree(d_breed_map);
+    cudaFree(d_mut_map);
+  }
+};
+
+// Per-GA device state: population buffers and two plan stages (the host draws
+// one while the device runs the other).
 struct DeviceGA {
-  Engine* e = nullptr;
   int P = 0, d = 0, window = 0, pairs_per_gen = 0, mut_cap = 0;
   float* d_pop = nullptr;
   float* d_sorted = nullptr;
   float* d_fit32 = nullptr;
   double* d_fit64 = nullptr;
   int* d_gen = nullptr;
-  // per plan buffer (two, so the host draws a window while the device runs the other)
   int* d_pairs[2] = {nullptr, nullptr};
   int* d_off[2] = {nullptr, nullptr};
   int* d_midx[2] = {nullptr, nullptr};
@@ -115,14 +178,10 @@ struct DeviceGA {
   int* h_midx[2] = {nullptr, nullptr};
   float* h_mval[2] = {nullptr, nullptr};
   float* h_hist[2] = {nullptr, nullptr};
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  cudaEvent_t done[2] = {nullptr, nullptr};
+  std::unique_ptr<GABatch> solo;  // the one-job batch of device_ga_advance
   std::vector<void*> dev, host;
   ~DeviceGA() {
-    for (int b = 0; b < 2; ++b) {
-      if (graph[b]) cudaGraphExecDestroy(graph[b]);
-      if (done[b]) cudaEventDestroy(done[b]);
-    }
+    solo.reset();
     for (void* p : dev) cudaFree(p);
     for (void* p : host) cudaFreeHost(p);
   }
@@ -141,6 +200,10 @@ struct DeviceGA {
 };
 
 void device_ga_free(DeviceGA* s) { delete s; }
+void ga_batch_free(GABatch* b) { delete b; }
+float* device_ga_population(DeviceGA* s) { return s->d_pop; }
+double* device_ga_fitness64(DeviceGA* s) { return s->d_fit64; }
+const float* device_ga_history(const DeviceGA* s, int b) { return s->h_hist[b]; }
 
 int device_rank(int device, int P, const double* fitness, int* order, float* sorted) {
   if (P < 1 || P > kMaxDevicePopulation) {
@@ -156,10 +219,9 @@ int device_rank(int device, int P, const double* fitness, int* order, float* sor
   if (ce == cudaSuccess) ce = cudaMalloc(&d_sorted, sizeof(float) * P);
   if (ce == cudaSuccess) ce = cudaMemcpy(d_fit, fitness, sizeof(double) * P, cudaMemcpyHostToDevice);
   if (ce == cudaSuccess && sizeof(float) * P > 48 * 1024)
-    ce = cudaFuncSetAttribute(ga_rank, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(float) * P));
+    ce = cudaFuncSetAttribute(ga_rank_values, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(float) * P));
   if (ce == cudaSuccess) {
-    ga_rank<<<(P + 255) / 256, 256, sizeof(float) * P>>>(P, 0, d_fit, nullptr, nullptr, d_sorted, nullptr, nullptr,
-                                                         d_order);
+    ga_rank_values<<<(P + kGABlock - 1) / kGABlock, kGABlock, sizeof(float) * P>>>(P, d_fit, d_sorted, d_order);
     ce = cudaGetLastError();
   }
   if (ce == cudaSuccess) ce = cudaMemcpy(order, d_order, sizeof(int) * P, cudaMemcpyDeviceToHost);
@@ -171,12 +233,14 @@ int device_rank(int device, int P, const double* fitness, int* order, float* sor
   return GPUGA_OK;
 }
 
-namespace {
-
-int setup(Engine* e, const GA& ga, int window, DeviceGA** out) {
+int device_ga_setup(const GA& ga, int window, DeviceGA** out) {
+  const int P = ga.gp.population_size;
+  if (P > kMaxDevicePopulation) {
+    set_error("the device GA loop supports populations up to %d (got %d).", kMaxDevicePopulation, P);
+    return GPUGA_ERR_UNSUPPORTED;
+  }
   std::unique_ptr<DeviceGA> s(new DeviceGA);
-  s->e = e;
-  s->P = ga.gp.population_size;
+  s->P = P;
   s->d = ga.d;
   s->window = window;
   s->pairs_per_gen = ga.child_number / 2;
@@ -200,35 +264,88 @@ int setup(Engine* e, const GA& ga, int window, DeviceGA** out) {
     GPUGA_TRY(s->halloc(&s->h_midx[b], nm));
     GPUGA_TRY(s->halloc(&s->h_mval[b], nm));
     GPUGA_TRY(s->halloc(&s->h_hist[b], nh));
-    GPUGA_CUDA(cudaEventCreateWithFlags(&s->done[b], cudaEventDisableTiming));
   }
-  const size_t rank_smem = sizeof(float) * s->P;
-  if (rank_smem > 48 * 1024)
-    GPUGA_CUDA(cudaFuncSetAttribute(ga_rank, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rank_smem));
   *out = s.release();
   return GPUGA_OK;
 }
 
-// One generation on buffer b: fitness of d_pop, then rank, breed, mutate, advance.
-int enqueue_one(DeviceGA* s, LaunchSet* ls, int b, cudaStream_t st) {
-  GPUGA_TRY(launchset_enqueue(ls, st));
-  const int P = s->P, d = s->d;
-  ga_rank<<<(P + 255) / 256, 256, sizeof(float) * P, st>>>(P, d, s->d_fit64, s->d_pop, s->d_sorted, s->d_fit32,
-                                                          s->d_hist[b], s->d_gen, nullptr);
+namespace {
+
+int enqueue_generation(GABatch* B, int b, cudaStream_t st) {
+  GPUGA_TRY(launchset_enqueue(B->ls, st));
+  ga_rank_jobs<<<B->n_rank, kGABlock, B->rank_smem, st>>>(B->d_table[b], B->d_rank_map);
   GPUGA_CUDA(cudaGetLastError());
-  const long long Pd = (long long)P * d;
-  ga_breed<<<(unsigned)((Pd + 255) / 256), 256, 0, st>>>(P, d, P - 2 * s->pairs_per_gen, s->d_pairs[b],
-                                                         s->pairs_per_gen, s->d_sorted, s->d_pop, s->d_gen);
+  ga_breed_jobs<<<B->n_breed, kGABlock, 0, st>>>(B->d_table[b], B->d_breed_map);
   GPUGA_CUDA(cudaGetLastError());
-  ga_mutate<<<(s->mut_cap + 255) / 256, 256, 0, st>>>(s->d_off[b], s->d_midx[b], s->d_mval[b], s->d_pop, s->d_gen);
+  ga_mutate_jobs<<<B->n_mut, kGABlock, 0, st>>>(B->d_table[b], B->d_mut_map);
   GPUGA_CUDA(cudaGetLastError());
-  ga_advance<<<1, 1, 0, st>>>(s->d_gen);
+  ga_advance_jobs<<<1, 128, 0, st>>>(B->d_table[b], (int)B->jobs.size());
   GPUGA_CUDA(cudaGetLastError());
   return GPUGA_OK;
 }
 
-// Draws generations [g0, g0 + n) into host buffer b.
-void draw_window(GA& ga, DeviceGA* s, int b, int g0, int n) {
+}  // namespace
+
+int ga_batch_build(const std::vector<DeviceGA*>& jobs, LaunchSet* ls, GABatch** out) {
+  std::unique_ptr<GABatch> B(new GABatch);
+  B->jobs = jobs;
+  B->ls = ls;
+  std::vector<int> rmap, bmap, mmap;
+  std::vector<GAJob> rows[2];
+  int maxP = 1;
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    const DeviceGA* s = jobs[j];
+    maxP = std::max(maxP, s->P);
+    GAJob row{};
+    row.P = s->P;
+    row.d = s->d;
+    row.parent_number = s->P - 2 * s->pairs_per_gen;
+    row.pairs_per_gen = s->pairs_per_gen;
+    row.rank_block0 = (int)rmap.size();
+    row.breed_block0 = (int)bmap.size();
+    row.mut_block0 = (int)mmap.size();
+    const long long Pd = (long long)s->P * s->d;
+    for (int k = 0; k < (s->P + kGABlock - 1) / kGABlock; ++k) rmap.push_back((int)j);
+    for (long long k = 0; k < (Pd + kGABlock - 1) / kGABlock; ++k) bmap.push_back((int)j);
+    for (int k = 0; k < (s->mut_cap + kGABlock - 1) / kGABlock; ++k) mmap.push_back((int)j);
+    row.pop = s->d_pop;
+    row.sorted = s->d_sorted;
+    row.fit32 = s->d_fit32;
+    row.fit64 = s->d_fit64;
+    row.gen = s->d_gen;
+    for (int b = 0; b < 2; ++b) {
+      GAJob r = row;
+      r.hist = s->d_hist[b];
+      r.pairs = s->d_pairs[b];
+      r.off = s->d_off[b];
+      r.midx = s->d_midx[b];
+      r.mval = s->d_mval[b];
+      rows[b].push_back(r);
+    }
+  }
+  B->n_rank = (int)rmap.size();
+  B->n_breed = (int)bmap.size();
+  B->n_mut = (int)mmap.size();
+  B->rank_smem = sizeof(float) * maxP;
+  GPUGA_CUDA(cudaMalloc(&B->d_rank_map, sizeof(int) * std::max<size_t>(rmap.size(), 1)));
+  GPUGA_CUDA(cudaMalloc(&B->d_breed_map, sizeof(int) * std::max<size_t>(bmap.size(), 1)));
+  GPUGA_CUDA(cudaMalloc(&B->d_mut_map, sizeof(int) * std::max<size_t>(mmap.size(), 1)));
+  GPUGA_CUDA(cudaMemcpy(B->d_rank_map, rmap.data(), sizeof(int) * rmap.size(), cudaMemcpyHostToDevice));
+  GPUGA_CUDA(cudaMemcpy(B->d_breed_map, bmap.data(), sizeof(int) * bmap.size(), cudaMemcpyHostToDevice));
+  GPUGA_CUDA(cudaMemcpy(B->d_mut_map, mmap.data(), sizeof(int) * mmap.size(), cudaMemcpyHostToDevice));
+  for (int b = 0; b < 2; ++b) {
+    GPUGA_CUDA(cudaMalloc(&B->d_table[b], sizeof(GAJob) * std::max<size_t>(jobs.size(), 1)));
+    GPUGA_CUDA(cudaMemcpy(B->d_table[b], rows[b].data(), sizeof(GAJob) * jobs.size(), cudaMemcpyHostToDevice));
+    GPUGA_CUDA(cudaEventCreateWithFlags(&B->done[b], cudaEventDisableTiming));
+  }
+  if (B->rank_smem > 48 * 1024)
+    GPUGA_CUDA(cudaFuncSetAttribute(ga_rank_jobs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->rank_smem));
+  *out = B.release();
+  return GPUGA_OK;
+}
+
+// Draws generations [g0, g0 + n) of `ga` into its host plan buffer b.
+void device_ga_draw(GA& ga, DeviceGA* s, int b, int g0, int n) {
   GenPlan plan;
   int moff = 0;
   s->h_off[b][0] = 0;
@@ -243,7 +360,7 @@ void draw_window(GA& ga, DeviceGA* s, int b, int g0, int n) {
   }
 }
 
-int upload_window(DeviceGA* s, int b, int n, cudaStream_t st) {
+int device_ga_upload(DeviceGA* s, int b, int n, cudaStream_t st) {
   GPUGA_CUDA(cudaMemcpyAsync(s->d_pairs[b], s->h_pairs[b], sizeof(int) * (size_t)n * s->pairs_per_gen * 3,
                              cudaMemcpyHostToDevice, st));
   GPUGA_CUDA(cudaMemcpyAsync(s->d_off[b], s->h_off[b], sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
@@ -255,43 +372,70 @@ int upload_window(DeviceGA* s, int b, int n, cudaStream_t st) {
   return GPUGA_OK;
 }
 
-int run_window(DeviceGA* s, LaunchSet* ls, int b, int n, bool use_graph, cudaStream_t st) {
-  GPUGA_CUDA(cudaMemsetAsync(s->d_gen, 0, sizeof(int), st));
-  if (use_graph && !s->graph[b]) {
+// n generations of every job of the batch on plan buffer b (uploaded before), then the
+// generation histories back to the host; done[b] marks the end.  With `timed`, events
+// bracket every generation (ga_batch_generation_ms).
+int ga_batch_window(GABatch* B, int b, int n, bool use_graph, bool timed, cudaStream_t st) {
+  for (DeviceGA* s : B->jobs) GPUGA_CUDA(cudaMemsetAsync(s->d_gen, 0, sizeof(int), st));
+  if (use_graph && !B->graph[b]) {
     cudaGraph_t g = nullptr;
     GPUGA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_one(s, ls, b, st);
+    int rc = enqueue_generation(B, b, st);
     cudaError_t ce = cudaStreamEndCapture(st, &g);
     if (rc != GPUGA_OK) {
       if (g) cudaGraphDestroy(g);
       return rc;
     }
     GPUGA_CUDA(ce);
-    cudaError_t ie = cudaGraphInstantiate(&s->graph[b], g, 0);
+    cudaError_t ie = cudaGraphInstantiate(&B->graph[b], g, 0);
     cudaGraphDestroy(g);
     GPUGA_CUDA(ie);
   }
+  while (timed && (int)B->gen_ev.size() < n + 1) {
+    cudaEvent_t e;
+    GPUGA_CUDA(cudaEventCreate(&e));
+    B->gen_ev.push_back(e);
+  }
+  if (timed) GPUGA_CUDA(cudaEventRecord(B->gen_ev[0], st));
   for (int k = 0; k < n; ++k) {
     if (use_graph) {
-      GPUGA_CUDA(cudaGraphLaunch(s->graph[b], st));
+      GPUGA_CUDA(cudaGraphLaunch(B->graph[b], st));
     } else {
-      GPUGA_TRY(enqueue_one(s, ls, b, st));
+      GPUGA_TRY(enqueue_generation(B, b, st));
     }
+    if (timed) GPUGA_CUDA(cudaEventRecord(B->gen_ev[k + 1], st));
   }
-  GPUGA_CUDA(cudaMemcpyAsync(s->h_hist[b], s->d_hist[b], sizeof(float) * (size_t)n * (s->d + 1),
-                             cudaMemcpyDeviceToHost, st));
-  GPUGA_CUDA(cudaEventRecord(s->done[b], st));
+  for (DeviceGA* s : B->jobs)
+    GPUGA_CUDA(cudaMemcpyAsync(s->h_hist[b], s->d_hist[b], sizeof(float) * (size_t)n * (s->d + 1),
+                               cudaMemcpyDeviceToHost, st));
+  GPUGA_CUDA(cudaEventRecord(B->done[b], st));
   return GPUGA_OK;
 }
 
-void emit_lines(const GA& ga, const DeviceGA* s, int b, int g0, int n, std::string* lines) {
-  for (int k = 0; k < n; ++k) {
-    const float* h = s->h_hist[b] + (size_t)k * (s->d + 1);
-    *lines += ga_output_line(g0 + k, h[0], h + 1, ga.pmin.data(), ga.pmax.data(), s->d);
-  }
+int ga_batch_wait(GABatch* B, int b) {
+  GPUGA_CUDA(cudaEventSynchronize(B->done[b]));
+  return GPUGA_OK;
 }
 
-}  // namespace
+int ga_batch_generation_ms(GABatch* B, int n, std::vector<double>* ms) {
+  for (int k = 0; k < n; ++k) {
+    float t = 0.f;
+    GPUGA_CUDA(cudaEventElapsedTime(&t, B->gen_ev[k], B->gen_ev[k + 1]));
+    ms->push_back(t);
+  }
+  return GPUGA_OK;
+}
+
+// Copies the device population and sorted fitness back into the host GA after
+// `generations` device generations.
+int device_ga_sync_host(GA* ga, DeviceGA* s, int generations, cudaStream_t st) {
+  GPUGA_CUDA(cudaMemcpyAsync(ga->population.data(), s->d_pop, sizeof(float) * (size_t)s->P * s->d,
+                             cudaMemcpyDeviceToHost, st));
+  GPUGA_CUDA(cudaMemcpyAsync(ga->fitness.data(), s->d_fit32, sizeof(float) * s->P, cudaMemcpyDeviceToHost, st));
+  GPUGA_CUDA(cudaStreamSynchronize(st));
+  ga->generation += generations;
+  return GPUGA_OK;
+}
 
 int device_ga_advance(Engine* e, GA* ga, DeviceGA** state, int generations, int window,
                       const std::function<void(const std::string&)>& sink) {
@@ -300,10 +444,6 @@ int device_ga_advance(Engine* e, GA* ga, DeviceGA** state, int generations, int 
     return GPUGA_ERR_ARG;
   }
   const int P = ga->gp.population_size;
-  if (P > kMaxDevicePopulation) {
-    set_error("the device GA loop supports populations up to %d (got %d).", kMaxDevicePopulation, P);
-    return GPUGA_ERR_UNSUPPORTED;
-  }
   if (window < 1) window = 32;
   generations = std::min(generations, ga->gp.maximum_generation - ga->generation);
   if (generations <= 0) return GPUGA_OK;
@@ -314,7 +454,7 @@ int device_ga_advance(Engine* e, GA* ga, DeviceGA** state, int generations, int 
     s = *state = nullptr;
   }
   if (!s) {
-    GPUGA_TRY(setup(e, *ga, window, &s));
+    GPUGA_TRY(device_ga_setup(*ga, window, &s));
     *state = s;
   }
   window = s->window;
@@ -322,6 +462,12 @@ int device_ga_advance(Engine* e, GA* ga, DeviceGA** state, int generations, int 
   Plan* plan = nullptr;
   GPUGA_TRY(plan_get(e, P, &plan));
   LaunchSet* ls = plan->ls.get();
+  if (!s->solo || s->solo->ls != ls) {
+    GABatch* B = nullptr;
+    GPUGA_TRY(ga_batch_build({s}, ls, &B));
+    s->solo.reset(B);
+  }
+  GABatch* B = s->solo.get();
   GPUGA_TRY(launchset_retarget(ls, 0, s->d_pop, s->d_fit64, nullptr, st));
   const bool use_graph = e->opt.use_graph && !ls->timing;
   GPUGA_CUDA(cudaMemcpyAsync(s->d_pop, ga->population.data(), sizeof(float) * (size_t)P * s->d,
@@ -329,31 +475,29 @@ int device_ga_advance(Engine* e, GA* ga, DeviceGA** state, int generations, int 
 
   // window k runs on buffer k % 2; the host draws window k + 1 while the device runs window k
   const int g_start = ga->generation;
-  int nwin = (generations + window - 1) / window;
+  const int nwin = (generations + window - 1) / window;
   auto wlen = [&](int k) { return std::min(window, generations - k * window); };
-  draw_window(*ga, s, 0, g_start, wlen(0));
-  GPUGA_TRY(upload_window(s, 0, wlen(0), st));
-  GPUGA_TRY(run_window(s, ls, 0, wlen(0), use_graph, st));
+  device_ga_draw(*ga, s, 0, g_start, wlen(0));
+  GPUGA_TRY(device_ga_upload(s, 0, wlen(0), st));
+  GPUGA_TRY(ga_batch_window(B, 0, wlen(0), use_graph, false, st));
   for (int k = 0; k < nwin; ++k) {
     const int b = k & 1;
     if (k + 1 < nwin) {
       // buffer b^1 was last read by window k - 1, which finished before window k started
-      if (k >= 1) GPUGA_CUDA(cudaEventSynchronize(s->done[b ^ 1]));
-      draw_window(*ga, s, b ^ 1, g_start + (k + 1) * window, wlen(k + 1));
-      GPUGA_TRY(upload_window(s, b ^ 1, wlen(k + 1), st));
-      GPUGA_TRY(run_window(s, ls, b ^ 1, wlen(k + 1), use_graph, st));
+      if (k >= 1) GPUGA_TRY(ga_batch_wait(B, b ^ 1));
+      device_ga_draw(*ga, s, b ^ 1, g_start + (k + 1) * window, wlen(k + 1));
+      GPUGA_TRY(device_ga_upload(s, b ^ 1, wlen(k + 1), st));
+      GPUGA_TRY(ga_batch_window(B, b ^ 1, wlen(k + 1), use_graph, false, st));
     }
-    GPUGA_CUDA(cudaEventSynchronize(s->done[b]));
+    GPUGA_TRY(ga_batch_wait(B, b));
     std::string lines;
-    emit_lines(*ga, s, b, g_start + k * window, wlen(k), &lines);
+    for (int q = 0; q < wlen(k); ++q) {
+      const float* h = s->h_hist[b] + (size_t)q * (s->d + 1);
+      lines += ga_output_line(g_start + k * window + q, h[0], h + 1, ga->pmin.data(), ga->pmax.data(), s->d);
+    }
     if (sink) sink(lines);
   }
-  GPUGA_CUDA(cudaMemcpyAsync(ga->population.data(), s->d_pop, sizeof(float) * (size_t)P * s->d,
-                             cudaMemcpyDeviceToHost, st));
-  GPUGA_CUDA(cudaMemcpyAsync(ga->fitness.data(), s->d_fit32, sizeof(float) * P, cudaMemcpyDeviceToHost, st));
-  GPUGA_CUDA(cudaStreamSynchronize(st));
-  ga->generation = g_start + generations;
-  return GPUGA_OK;
+  return device_ga_sync_host(ga, s, generations, st);
 }
 
 }  // namespace gpuga

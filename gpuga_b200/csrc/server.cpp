@@ -3,15 +3,18 @@
 // A scheduler thread owns the device.  Jobs are admitted in arrival order as
 // long as the sum of their device footprints stays within the HBM budget and
 // the number of resident jobs is below max_jobs; every resident job keeps its
-// training set, population buffers and per-(individual, configuration)
-// results on the GPU.  Each scheduler tick runs ONE generation of EVERY
-// resident job: the populations go up, a single launch set (one decode, the
-// shared batched force launches whose work items come from all jobs, one
-// fitness fold) evaluates them, the fitness vectors come back, and each job's
-// GA takes its step on the host.  Jobs that arrive while others run join at
-// the next tick boundary; finished or cancelled jobs leave and free their
-// memory.  Work items of different jobs never share a CTA and all reductions
-// are fixed-order, so a job's trajectory is identical alone and in any mix.
+// training set, population and GA buffers and per-(individual, configuration)
+// results on the GPU.  The scheduler advances all resident jobs together in
+// windows of up to kWindow generations.  Each generation is one CUDA graph: a
+// single launch set (one decode, the shared batched force launches whose work
+// items come from all jobs, one fitness fold) evaluates every job's
+// population, then the batched GA kernels (ga_device.cu) select, cross over
+// and mutate every job's population from random choices the host drew for the
+// window in advance -- no population or fitness crosses PCIe between
+// generations.  Jobs that arrive while others run join at the next window
+// boundary; finished or cancelled jobs leave and free their memory.  Work
+// items of different jobs never share a CTA and all reductions are
+// fixed-order, so a job's trajectory is identical alone and in any mix.
 // There is no counterpart in the reference, which fits one potential per
 // process (main.cu:25-55).
 #include <algorithm>
@@ -56,7 +59,8 @@ struct Job {
   // run state
   Plan* plan = nullptr;             // the job's own buffers (owned by plan_owner)
   std::unique_ptr<Plan> plan_owner;
-  GA ga;
+  GA ga;                            // host side: random stream and plan draws
+  std::unique_ptr<DeviceGA, void (*)(DeviceGA*)> dga{nullptr, device_ga_free};
   int gens_total = 0;
   std::vector<float> best;
   std::vector<float> elite;
@@ -88,6 +92,10 @@ size_t estimate_bytes(const PotentialSpec& spec, const TrainingSet& ts, int P) {
 
 }  // namespace
 
+// Generations per scheduling window (admission, retirement and cancellation
+// happen at window boundaries).
+constexpr int kWindow = 8;
+
 struct gpuga_server {
   int device = 0;
   double budget = 0;
@@ -104,9 +112,10 @@ struct gpuga_server {
   std::thread worker;
   cudaStream_t st = nullptr;
   std::unique_ptr<LaunchSet> ls;
+  std::unique_ptr<GABatch, void (*)(GABatch*)> gab{nullptr, ga_batch_free};
   std::vector<int> ls_ids;
   // statistics
-  std::vector<double> tick_ms;
+  std::vector<double> tick_ms;  // device time of each generation (all resident jobs)
   long batches = 0, finished = 0;
   double evals = 0, busy_s = 0;
   int peak_resident = 0;
@@ -114,7 +123,7 @@ struct gpuga_server {
 
   void run();
   bool admit_locked(std::unique_lock<std::mutex>& lock);
-  int tick();
+  int window();
   void finish(Job* j, int state, int status, const char* msg);
 };
 
@@ -123,6 +132,7 @@ void gpuga_server::finish(Job* j, int state, int status, const char* msg) {
   j->status = status;
   if (msg) j->error = msg;
   j->t_end = Clock::now();
+  j->dga.reset();
   j->plan_owner.reset();
   j->plan = nullptr;
   if (j->engine && !j->shared) delete j->engine;
@@ -166,6 +176,16 @@ bool gpuga_server::admit_locked(std::unique_lock<std::mutex>& lock) {
     if (s == GPUGA_OK)
       s = j->ga.init(j->engine->spec.num_vars, j->engine->spec.pmin.data(), j->engine->spec.pmax.data(), j->gp,
                      j->seed);
+    if (s == GPUGA_OK) {
+      DeviceGA* g = nullptr;
+      s = device_ga_setup(j->ga, kWindow, &g);
+      j->dga.reset(g);
+    }
+    if (s == GPUGA_OK) {
+      const cudaError_t ce = cudaMemcpy(device_ga_population(j->dga.get()), j->ga.population.data(),
+                                        sizeof(float) * j->ga.population.size(), cudaMemcpyHostToDevice);
+      if (ce != cudaSuccess) s = cuda_status(ce, "cudaMemcpy", __FILE__, __LINE__);
+    }
     lock.lock();
     if (s != GPUGA_OK) {
       finish(j, kFailed, s, last_error());
@@ -178,45 +198,52 @@ bool gpuga_server::admit_locked(std::unique_lock<std::mutex>& lock) {
   return changed;
 }
 
-// One generation of every resident job through one launch set.
-int gpuga_server::tick() {
+// Up to kWindow generations of every resident job: shared fitness launches and
+// batched GA kernels per generation, one CUDA graph, no host round trip.
+int gpuga_server::window() {
   std::vector<int> ids;
   for (Job* j : running) ids.push_back(j->id);
   if (!ls || ids != ls_ids) {
+    gab.reset();
     std::vector<std::pair<Engine*, Plan*>> v;
-    for (Job* j : running) v.push_back({j->engine, j->plan});
+    std::vector<DeviceGA*> g;
+    for (Job* j : running) {
+      v.push_back({j->engine, j->plan});
+      g.push_back(j->dga.get());
+    }
     ls.reset(new LaunchSet);
     GPUGA_TRY(launchset_build(v, ls.get()));
+    for (size_t k = 0; k < running.size(); ++k)
+      GPUGA_TRY(launchset_retarget(ls.get(), (int)k, device_ga_population(g[k]), device_ga_fitness64(g[k]), nullptr,
+                                   st));
+    GABatch* b = nullptr;
+    GPUGA_TRY(ga_batch_build(g, ls.get(), &b));
+    gab.reset(b);
     ls_ids = ids;
   }
+  int n = kWindow;
+  for (Job* j : running) n = std::min(n, j->gens_total - j->ga.generation);
+  if (n <= 0) return GPUGA_OK;
   const auto t0 = Clock::now();
-  for (size_t k = 0; k < running.size(); ++k) {
-    Job* j = running[k];
-    Plan* p = j->plan;
-    const size_t n = (size_t)p->P * j->engine->d.num_vars;
-    memcpy(p->h_pop, j->ga.population.data(), sizeof(float) * n);
-    GPUGA_CUDA(cudaMemcpyAsync(p->d_pop, p->h_pop, sizeof(float) * n, cudaMemcpyHostToDevice, st));
-    GPUGA_TRY(launchset_retarget(ls.get(), (int)k, p->d_pop, p->d_fitness, nullptr, st));
-  }
-  GPUGA_TRY(launchset_enqueue(ls.get(), st));
-  for (Job* j : running)
-    GPUGA_CUDA(cudaMemcpyAsync(j->plan->h_fit, j->plan->d_fitness, sizeof(double) * j->plan->P,
-                               cudaMemcpyDeviceToHost, st));
-  GPUGA_CUDA(cudaStreamSynchronize(st));
   for (Job* j : running) {
-    const double* fit = j->plan->h_fit;
-    j->ga.eval = [fit](int P, const float*, float* out) {
-      for (int q = 0; q < P; ++q) out[q] = (float)fit[q];  // the reference ranks FP32 fitness values
-      return GPUGA_OK;
-    };
-    GPUGA_TRY(j->ga.step(nullptr));
-    j->best.push_back(j->ga.fitness[0]);
-    evals += (double)j->plan->P * j->engine->d.N;
+    device_ga_draw(j->ga, j->dga.get(), 0, j->ga.generation, n);
+    GPUGA_TRY(device_ga_upload(j->dga.get(), 0, n, st));
   }
-  const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
-  tick_ms.push_back(ms);
-  busy_s += ms * 1e-3;
-  ++batches;
+  GPUGA_TRY(ga_batch_window(gab.get(), 0, n, true, true, st));
+  GPUGA_TRY(ga_batch_wait(gab.get(), 0));
+  std::vector<double> ms;
+  GPUGA_TRY(ga_batch_generation_ms(gab.get(), n, &ms));
+  for (Job* j : running) {
+    const float* h = device_ga_history(j->dga.get(), 0);
+    for (int q = 0; q < n; ++q) j->best.push_back(h[(size_t)q * (j->ga.d + 1)]);
+    j->ga.generation += n;
+    evals += (double)j->plan->P * j->engine->d.N * n;
+  }
+  // latency: device time of each generation; throughput: wall time of the window (plan draws,
+  // uploads and the history read-back included)
+  for (double t : ms) tick_ms.push_back(t);
+  busy_s += std::chrono::duration<double>(Clock::now() - t0).count();
+  batches += n;
   return GPUGA_OK;
 }
 
@@ -238,9 +265,9 @@ void gpuga_server::run() {
       continue;
     }
     lock.unlock();
-    const int s = tick();
+    const int s = window();
     lock.lock();
-    // retire finished, failed and cancelled jobs at the tick boundary
+    // retire finished, failed and cancelled jobs at the window boundary
     std::vector<Job*> keep;
     for (Job* j : running) {
       if (s != GPUGA_OK) {
@@ -248,6 +275,12 @@ void gpuga_server::run() {
       } else if (j->cancel_requested) {
         finish(j, kCancelled, GPUGA_ERR_CANCELLED, "cancelled");
       } else if (j->ga.generation >= j->gens_total) {
+        // the final population (row 0 = the last generation's elite) comes back once
+        const int ss = device_ga_sync_host(&j->ga, j->dga.get(), 0, st);
+        if (ss != GPUGA_OK) {
+          finish(j, kFailed, ss, last_error());
+          continue;
+        }
         j->elite.assign(j->ga.population.begin(), j->ga.population.begin() + j->ga.d);
         finish(j, kDone, GPUGA_OK, nullptr);
       } else {
@@ -257,6 +290,7 @@ void gpuga_server::run() {
     running.swap(keep);
     if (s != GPUGA_OK) worker_status = s;
   }
+  gab.reset();
   ls.reset();
   cudaStreamDestroy(st);
   st = nullptr;

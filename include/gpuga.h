@@ -223,8 +223,10 @@ int gpuga_neighbor_compute(int Nc, int N, int max_Na, const int* Na, const int* 
 /* ------------------------------------------------------------------ serving */
 /* A device-resident server that runs many fitting jobs concurrently, admitting jobs while the
  * sum of their device footprints stays within hbm_budget_bytes and batching the generations of
- * all running jobs into shared launches.  No reference counterpart (the reference fits one
- * potential per process, main.cu:25-55). */
+ * all running jobs into shared launches: fitness and GA (selection, crossover, mutation) of every
+ * resident job run on the GPU, up to 8 generations per scheduling window, from random choices the
+ * host draws from each job's own std::mt19937 stream.  Jobs join and leave at window boundaries.
+ * No reference counterpart (the reference fits one potential per process, main.cu:25-55). */
 int gpuga_server_create(int device, double hbm_budget_bytes, int max_jobs, gpuga_server** out);
 /* Submits a fitting job for <dir> (potential.in, train.in, ga.in).  generations <= 0 uses ga.in.
  * Returns the job id in *job_id. */
@@ -240,8 +242,9 @@ int gpuga_server_result(gpuga_server* s, int job_id, float* best_out, float* eli
 int gpuga_server_cancel(gpuga_server* s, int job_id);
 /* Runs the scheduler until every submitted job is finished (or timeout_s elapses, -> GPUGA_ERR_TIMEOUT). */
 int gpuga_server_drain(gpuga_server* s, double timeout_s);
-/* stats: {generation batches run, jobs finished, p50 gen latency ms, p99 gen latency ms,
- *         aggregate evals/s, device bytes in use, peak jobs resident, total evals} */
+/* stats: {generation batches run, jobs finished, p50 and p99 of the device time of a generation of all
+ *         resident jobs (ms), aggregate evals/s over the windows' wall time, device bytes in use,
+ *         peak jobs resident, total evals} */
 int gpuga_server_stats(gpuga_server* s, double* stats8);
 int gpuga_server_destroy(gpuga_server* s);
 
