@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cmath>
 #include <tuple>
+#include <type_traits>
 
 #include <cuda_pipeline.h>
 
@@ -514,18 +515,15 @@ __device__ __forceinline__ float exp_neg_dd(float xh, float xl, float yh, float 
   return fmaf(-lo, e, e);
 }
 
-__device__ __forceinline__ void ri_pair(const RIC& R, int t, float d, float4 w, float& p2, float& fd) {
-  const float a = t == 0 ? R.a[0] : (t == 1 ? R.a[1] : R.a[2]);
-  const float b = t == 0 ? R.b[0] : (t == 1 ? R.b[1] : R.b[2]);
-  const float blo = t == 0 ? R.blo[0] : (t == 1 ? R.blo[1] : R.blo[2]);
-  const float c = t == 0 ? R.c[0] : (t == 1 ? R.c[1] : R.c[2]);
-  const float c6 = t == 0 ? R.c6[0] : (t == 1 ? R.c6[1] : R.c6[2]);
-  const float qq = t == 0 ? R.qq[0] : (t == 1 ? R.qq[1] : R.qq[2]);
+// Pair type T (0 cation-cation, 1 cation-anion with Morse, 2 anion-anion) at compile time:
+// the lane's constants of that type stay in registers and the Morse terms exist only for T = 1.
+template <int T>
+__device__ __forceinline__ void ri_pair(const RIC& R, float d, float4 w, float& p2, float& fd) {
   const float dlo = w.x;
-  const float ex = exp_neg_dd(d, dlo, b, blo);
-  p2 = a * ex - c * w.y + qq * (w.z - R.vrc - R.dvrc * (d - R.rc));
-  fd = __fdividef(c6 * w.y, d) - a * ex * b - qq * (w.w + R.dvrc);
-  if (t == 1) {
+  const float ex = exp_neg_dd(d, dlo, R.b[T], R.blo[T]);
+  p2 = R.a[T] * ex - R.c[T] * w.y + R.qq[T] * (w.z - R.vrc - R.dvrc * (d - R.rc));
+  fd = __fdividef(R.c6[T] * w.y, d) - R.a[T] * ex * R.b[T] - R.qq[T] * (w.w + R.dvrc);
+  if constexpr (T == 1) {
     // d - r0 as hi + lo (TwoSum), then the two Morse exponentials
     const float drh = d - R.r0;
     const float bb = drh - d;
@@ -537,13 +535,13 @@ __device__ __forceinline__ void ri_pair(const RIC& R, int t, float d, float4 w, 
   }
 }
 
-// Compensated FP32 sum (Kahan): the running error c is subtracted from each
-// new term; value() is the sum in FP64.  Error about 2 eps sum|x| for any
-// order of terms, against (n - 1) eps sum|x| for a plain FP32 sum.
 // bonds per chunk of the RI pair pipeline (one bond per lane); two stages per warp
 constexpr int kPairChunk = 32;
 constexpr size_t kPairStageBytes = (size_t)kWarps * 2 * 2 * kPairChunk * sizeof(float4);
 
+// Compensated FP32 sum (Kahan): the running error c is subtracted from each
+// new term; value() is the sum in FP64.  Error about 2 eps sum|x| for any
+// order of terms, against (n - 1) eps sum|x| for a plain FP32 sum.
 struct KSum {
   float s = 0.f, c = 0.f;
   __device__ __forceinline__ void add(float x) {
@@ -740,27 +738,37 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
     // chunk (possibly empty: force items still owe the atom's force error).
     float4* buf = reinterpret_cast<float4*>(smem + (size_t)kWarps * 32 * kResK * sizeof(double)) +
                   (size_t)warp * 4 * kPairChunk;  // [stage][geometry | Coulomb terms][kPairChunk]
-    int f_il = warp, f_b = 0, f_e = 0;
-    if (f_il < Na) bond_range(f_il, f_b, f_e);
-    int q_il[2], q_b[2], q_n[2], q_pt[2];
+    // the atom's pairs come grouped by pair type (rseg), so a chunk splits into at most three
+    // runs of one type each, evaluated with that type's constants hoisted
+    int4 f_seg = make_int4(0, 0, 0, 0);
+    int f_il = warp, f_b = 0;
+    if (f_il < Na) {
+      f_seg = S.rseg[atom0 + f_il];
+      f_b = f_seg.x;
+    }
+    int q_il[2], q_b[2], q_n[2], q_s1[2], q_s2[2];
     bool q_last[2], q_has[2];
     auto fetch = [&](int st) {
       q_has[st] = f_il < Na;
       if (!q_has[st]) return;
       q_il[st] = f_il;
       q_b[st] = f_b;
-      q_n[st] = min(kPairChunk, f_e - f_b);
+      q_n[st] = min(kPairChunk, f_seg.w - f_b);
+      q_s1[st] = f_seg.y;
+      q_s2[st] = f_seg.z;
       f_b += q_n[st];
-      q_last[st] = f_b >= f_e;
+      q_last[st] = f_b >= f_seg.w;
       if (q_last[st]) {
         f_il += kWarps;
-        if (f_il < Na) bond_range(f_il, f_b, f_e);
+        if (f_il < Na) {
+          f_seg = S.rseg[atom0 + f_il];
+          f_b = f_seg.x;
+        }
       }
       if (lane < q_n[st]) {
         const int bnd = q_b[st] + lane;
-        __pipeline_memcpy_async(buf + (2 * st) * kPairChunk + lane, S.g32 + bnd, sizeof(float4));
-        __pipeline_memcpy_async(buf + (2 * st + 1) * kPairChunk + lane, S.gri + bnd, sizeof(float4));
-        q_pt[st] = S.ptype[bnd];
+        __pipeline_memcpy_async(buf + (2 * st) * kPairChunk + lane, S.rg32 + bnd, sizeof(float4));
+        __pipeline_memcpy_async(buf + (2 * st + 1) * kPairChunk + lane, S.rgri + bnd, sizeof(float4));
       }
     };
     fetch(0);
@@ -772,14 +780,21 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
       __syncwarp();
       const float4* g = buf + (2 * st) * kPairChunk;
       const float4* w = g + kPairChunk;
-      const int n = q_n[st], pt = q_pt[st];
+      const int n = q_n[st], b0 = q_b[st];
+      const int k1 = min(max(q_s1[st] - b0, 0), n), k2 = min(max(q_s2[st] - b0, 0), n);
+      auto run = [&](auto type, int kb, int ke) {
+        constexpr int T = decltype(type)::value;
 #pragma unroll 2
-      for (int k = 0; k < n; ++k) {
-        const float4 q = g[k];
-        float p2, fd;
-        ri_pair(R, __shfl_sync(0xffffffffu, pt, k), q.w, w[k], p2, fd);
-        consume(ks, q, p2, fd);
-      }
+        for (int k = kb; k < ke; ++k) {
+          const float4 q = g[k];
+          float p2, fd;
+          ri_pair<T>(R, q.w, w[k], p2, fd);
+          consume(ks, q, p2, fd);
+        }
+      };
+      run(std::integral_constant<int, 0>{}, 0, k1);
+      run(std::integral_constant<int, 1>{}, k1, k2);
+      run(std::integral_constant<int, 2>{}, k2, n);
       if (q_last[st]) finish_atom(q_il[st], ks);
       __syncwarp();  // every lane is done with stage st before it is refilled
       fetch(st);
@@ -908,6 +923,9 @@ DevView make_view(const DevSet& d) {
   v.ptype = d.ptype;
   v.g32 = d.g32;
   v.gri = d.gri;
+  v.rg32 = d.rg32;
+  v.rgri = d.rgri;
+  v.rseg = d.rseg;
   v.force_ref = d.force_ref;
   return v;
 }

@@ -9,6 +9,7 @@
 //            g32[B] float4 (unit vector, d), g64[B] double4 (x,y,z,d),
 //            gri[B] float4 (RI: FP64 remainder of d, and the geometry-only terms 1/d^6 and the
 //            damped Coulomb energy / force pieces)
+//            RI: rg32 / rgri / rseg, each atom's evaluated pairs grouped by pair type
 //   targets  force_ref[3N], E_ref[Nc], W_ref[6Nc] (FP64 copies of the FP32 inputs)
 //
 // Bond vectors use the periodic image chosen by the reference's FP32 rule and
@@ -50,6 +51,12 @@ struct DevSet {
   float4* g32 = nullptr;
   double4* g64 = nullptr;
   float4* gri = nullptr;
+  // RI batched lists: per atom the pairs its work items evaluate (the full list for force
+  // configurations, the half list for energy/virial ones) grouped by pair type, in list order
+  // within a type: rseg[i] = (start, start of type 1, start of type 2, end) into rg32 / rgri
+  float4* rg32 = nullptr;
+  float4* rgri = nullptr;
+  int4* rseg = nullptr;
   float* force_ref = nullptr;
   double* E_ref = nullptr;
   double* W_ref = nullptr;
@@ -83,6 +90,9 @@ struct DevView {
   const uint8_t* ptype;
   const float4* g32;
   const float4* gri;
+  const float4* rg32;
+  const float4* rgri;
+  const int4* rseg;
   const float* force_ref;
 };
 

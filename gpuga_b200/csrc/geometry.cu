@@ -266,6 +266,29 @@ __global__ void reverse_slots(int N, const int* __restrict__ atom_cfg, const int
   }
 }
 
+// RI: each atom's evaluated pairs (full list for force configurations, i < N_force;
+// half list otherwise) copied grouped by pair type, list order kept within a type.
+__global__ void ri_group(int N, int N_force, const int* __restrict__ off, const int* __restrict__ half_off,
+                         const uint8_t* __restrict__ ptype, const float4* __restrict__ g32,
+                         const float4* __restrict__ gri, const int* __restrict__ start, float4* __restrict__ rg32,
+                         float4* __restrict__ rgri, int4* __restrict__ rseg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int bb = i < N_force ? off[i] : half_off[i], be = off[i + 1];
+  int o = start[i];
+  int seg[3];
+  for (int t = 0; t < 3; ++t) {
+    seg[t] = o;
+    for (int b = bb; b < be; ++b) {
+      if (ptype[b] != t) continue;
+      rg32[o] = g32[b];
+      rgri[o] = gri[b];
+      ++o;
+    }
+  }
+  rseg[i] = make_int4(seg[0], seg[1], seg[2], o);
+}
+
 // Bond geometry for lists in the reference layout NL[k*N + i]: the FP32 rule
 // picks the image, the vector is then evaluated in FP64; rev holds the slot of
 // the reverse bond (slot 0 of the neighbor when absent, minimal_tersoff.cu:368).
@@ -511,6 +534,24 @@ int build_geometry(Engine* e) {
   GPUGA_TRY(e->alloc(&d.rev_sm, std::max(B, 1)));
   reverse_slots<<<(N + 127) / 128, 128, 0, st>>>(N, d_atom_cfg, d.Na, d.Na_sum, d.off, d.nbr, d.rev, d.rev_sm);
   GPUGA_CUDA(cudaGetLastError());
+  if (d.potential_type == 0) {
+    std::vector<int> half(N), start(N + 1, 0);
+    GPUGA_CUDA(cudaMemcpyAsync(half.data(), d.half_off, sizeof(int) * N, cudaMemcpyDeviceToHost, st));
+    GPUGA_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < N; ++i)
+      start[i + 1] = start[i] + e->h_off[i + 1] - (i < ts.N_force ? e->h_off[i] : half[i]);
+    int* d_start = nullptr;
+    GPUGA_CUDA(cudaMalloc(&d_start, sizeof(int) * (N + 1)));
+    GPUGA_CUDA(cudaMemcpyAsync(d_start, start.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice, st));
+    GPUGA_TRY(e->alloc(&d.rg32, std::max(start[N], 1)));
+    GPUGA_TRY(e->alloc(&d.rgri, std::max(start[N], 1)));
+    GPUGA_TRY(e->alloc(&d.rseg, N));
+    ri_group<<<(N + 127) / 128, 128, 0, st>>>(N, ts.N_force, d.off, d.half_off, d.ptype, d.g32, d.gri, d_start, d.rg32,
+                                              d.rgri, d.rseg);
+    GPUGA_CUDA(cudaGetLastError());
+    GPUGA_CUDA(cudaStreamSynchronize(st));
+    cudaFree(d_start);
+  }
 
   GPUGA_CUDA(cudaStreamSynchronize(st));
   cudaFree(img);
