@@ -922,7 +922,6 @@ DevView make_view(const DevSet& d) {
   v.rev_sm = d.rev_sm;
   v.ptype = d.ptype;
   v.g32 = d.g32;
-  v.gri = d.gri;
   v.rg32 = d.rg32;
   v.rgri = d.rgri;
   v.rseg = d.rseg;

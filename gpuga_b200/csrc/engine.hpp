@@ -1,13 +1,13 @@
 // Engine: one training set resident in HBM plus the buffers of the batched
 // fitness evaluation.  Layout (all device arrays):
 //
-//   configs  Na[Nc], Na_sum[Nc], cfg_zmax[Nc]
+//   configs  Na[Nc], Na_sum[Nc], h[18 Nc] (FP32 box + inverse)
 //   atoms    type[N], r[3N] (SoA, FP32 as parsed), NN[N], off[N+1] (CSR into bonds),
 //            half_off[N] (first bond whose neighbor index is > i)
 //   bonds    nbr[B], rev[B] (reverse bond), rev_sm[B] (the reverse bond's slot * Na + atom,
 //            local to the configuration), ptype[B] (pair set / RI pair type),
-//            g32[B] float4 (unit vector, d), g64[B] double4 (x,y,z,d),
-//            gri[B] float4 (RI: FP64 remainder of d, and the geometry-only terms 1/d^6 and the
+//            g32[B] float4 (unit vector, d; not kept for RI), g64[B] double4 (x,y,z,d),
+//            gri[B] float4 (RI build scratch: FP64 remainder of d, 1/d^6 and the
 //            damped Coulomb energy / force pieces)
 //            RI: rg32 / rgri / rseg, each atom's evaluated pairs grouped by pair type
 //   targets  force_ref[3N], E_ref[Nc], W_ref[6Nc] (FP64 copies of the FP32 inputs)
@@ -50,7 +50,7 @@ struct DevSet {
   uint8_t* ptype = nullptr;
   float4* g32 = nullptr;
   double4* g64 = nullptr;
-  float4* gri = nullptr;
+  float4* gri = nullptr;   // RI build scratch (freed once rg32 / rgri exist)
   // RI batched lists: per atom the pairs its work items evaluate (the full list for force
   // configurations, the half list for energy/virial ones) grouped by pair type, in list order
   // within a type: rseg[i] = (start, start of type 1, start of type 2, end) into rg32 / rgri
@@ -89,7 +89,6 @@ struct DevView {
   const int* rev_sm;
   const uint8_t* ptype;
   const float4* g32;
-  const float4* gri;
   const float4* rg32;
   const float4* rgri;
   const int4* rseg;

@@ -516,11 +516,17 @@ int build_geometry(Engine* e) {
   GPUGA_CUDA(cudaMemcpyAsync(d_atom_cfg, atom_cfg.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
 
   GPUGA_TRY(e->alloc(&d.g64, std::max(B, 1)));
-  GPUGA_TRY(e->alloc(&d.g32, std::max(B, 1)));
+  // RI evaluates its type-grouped copies (rg32 / rgri, below): there g32 and gri are scratch
+  const bool ri = d.potential_type == 0;
+  if (ri) {
+    GPUGA_CUDA(cudaMalloc(&d.g32, sizeof(float4) * std::max(B, 1)));
+    GPUGA_CUDA(cudaMalloc(&d.gri, sizeof(float4) * std::max(B, 1)));
+  } else {
+    GPUGA_TRY(e->alloc(&d.g32, std::max(B, 1)));
+  }
   GPUGA_TRY(e->alloc(&d.rev, std::max(B, 1)));
   GPUGA_TRY(e->alloc(&d.half_off, N));
   GPUGA_TRY(e->alloc(&d.ptype, std::max(B, 1)));
-  if (d.potential_type == 0) GPUGA_TRY(e->alloc(&d.gri, std::max(B, 1)));
   double rc_fixed = 0.0;
   if (d.potential_type == 0 && e->spec.pmin.size() > 10 && e->spec.pmin[10] == e->spec.pmax[10] &&
       e->spec.pmin[10] > 0) {
@@ -551,6 +557,10 @@ int build_geometry(Engine* e) {
     GPUGA_CUDA(cudaGetLastError());
     GPUGA_CUDA(cudaStreamSynchronize(st));
     cudaFree(d_start);
+    cudaFree(d.g32);
+    cudaFree(d.gri);
+    d.g32 = nullptr;
+    d.gri = nullptr;
   }
 
   GPUGA_CUDA(cudaStreamSynchronize(st));
