@@ -155,35 +155,30 @@ def measured_peaks() -> dict:
         return {}
 
 
-def ncu_traffic(kernel: str, workload: int, units: float):
-    """DRAM bytes (read + write) of one launch of `kernel`, from the ncu capture summarised in
-    profiles/dram_traffic.md (lines `traffic: workload=W kernel=K units=U bytes=B`), or None
-    when that launch shape was not captured."""
+def _ncu_counts(tag: str):
+    """Lines `<tag>: key=value ...` of profiles/ncu_counts.txt (figures from ncu captures)."""
     try:
-        lines = open(os.path.join(ROOT, "profiles", "dram_traffic.md")).read().splitlines()
+        lines = open(os.path.join(ROOT, "profiles", "ncu_counts.txt")).read().splitlines()
     except OSError:
-        return None
-    for line in lines:
-        if not line.startswith("traffic:"):
-            continue
-        kv = dict(tok.split("=", 1) for tok in line.split()[1:])
+        return []
+    return [dict(tok.split("=", 1) for tok in ln.split()[1:]) for ln in lines if ln.startswith(tag + ":")]
+
+
+def ncu_traffic(kernel: str, workload: int, units: float):
+    """DRAM bytes (read + write) of one launch of `kernel` from an ncu capture of the same launch
+    shape, or None when that shape was not captured."""
+    for kv in _ncu_counts("traffic"):
         if int(kv["workload"]) == workload and kv["kernel"] == kernel and float(kv["units"]) == units:
             return float(kv["bytes"])
     return None
 
 
 def ncu_inst_per_unit(kernel: str, workload: int):
-    """Warp instructions per (individual, atom) of `kernel` from the ncu capture summarised in
-    profiles/tersoff_batched_mid_ncu.md (lines `inst: workload=W kernel=K warp_inst_per_unit=X`)."""
-    try:
-        lines = open(os.path.join(ROOT, "profiles", "tersoff_batched_mid_ncu.md")).read().splitlines()
-    except OSError:
-        return None
-    for line in lines:
-        if line.startswith("inst:"):
-            kv = dict(tok.split("=", 1) for tok in line.split()[1:])
-            if int(kv["workload"]) == workload and kv["kernel"] == kernel:
-                return float(kv["warp_inst_per_unit"])
+    """Warp instructions per (individual, atom) of `kernel` from an ncu capture (the work-item shapes,
+    hence the count per unit, depend on the configurations only)."""
+    for kv in _ncu_counts("inst"):
+        if int(kv["workload"]) == workload and kv["kernel"] == kernel:
+            return float(kv["warp_inst_per_unit"])
     return None
 
 
@@ -308,13 +303,17 @@ def run_ours(args, dist: Dist):
         achieved = ipu * dom["units"] / (dom["ms"] * 1e-3)
         peak = 4.0 * sms * mhz * 1e6
         issue = {"warp_inst_per_unit": ipu, "achieved_warp_inst_per_s": achieved, "peak_warp_inst_per_s": peak,
-                 "frac": achieved / peak, "source": "ncu smsp__inst_executed, profiles/tersoff_batched_mid_ncu.md"}
+                 "frac": achieved / peak, "source": "ncu smsp__inst_executed, profiles/ncu_counts.txt"}
     roofline = {"bound": "fp32", "kernel": dom["kernel"], "achieved": dom["tflops"], "peak": peak_fp32.value,
                 "unit": "TFLOP/s", "frac": dom["tflops"] / peak_fp32.value if dom["tflops"] else None,
                 "traffic": traffic, "peak_source": "measured: FFMA-chain calibration kernel on this GPU",
                 "algorithmic": "FP32 flops of the batched formulation (FMA=2), transcendentals separate",
                 "ms_per_launch": dom["ms"], "launches": launches,
                 "issue": issue,
+                "hbm": ({"achieved_gbs": traffic / (dom["ms"] * 1e-3) / 1e9,
+                         "peak_gbs": measured_peaks().get("hbm_gbs"),
+                         "frac": traffic / (dom["ms"] * 1e-3) / 1e9 / measured_peaks()["hbm_gbs"]}
+                        if traffic and dom["ms"] > 0 and measured_peaks().get("hbm_gbs") else None),
                 "generation": {"flops": gen_flops, "ms": ms_per_step,
                                "achieved": gen_flops / (ms_per_step * 1e-3) / 1e12,
                                "frac": gen_flops / (ms_per_step * 1e-3) / 1e12 / peak_fp32.value}}
