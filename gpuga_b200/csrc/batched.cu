@@ -7,20 +7,24 @@
 // for 32 individuals, G individuals x 32/G atoms.  With G = 32 a warp walks
 // one atom at a time for 32 parameter vectors: every geometry load is a
 // warp-uniform broadcast and the neighbor loops never diverge.  Per-lane
-// energy / virial / force-error sums stay in FP64 registers; a fixed-order
-// shared-memory reduction produces the (individual, configuration) results,
-// and a second kernel folds them into the weighted relative-RMSE fitness in a
-// fixed order, so a result never depends on what else shares the launch.
+// energy / virial / force-error sums are FP64 (registers, or shared memory for
+// the Tersoff energy/virial CTAs); a fixed-order shared-memory reduction
+// produces the (individual, configuration) results, and a second kernel folds
+// them into the weighted relative-RMSE fitness in a fixed order, so a result
+// never depends on what else shares the launch.
 //
 // Precision.  Pair, bond-order and three-body arithmetic is FP32 on CUDA cores
-// (accurate libdevice exp/erfc/tanh, the bond-order power with a double-float
-// exponent (powf_dd.cuh), no fast-math); site energies and
-// virials are summed per atom in FP32 and across atoms in FP64; the loss and
+// (accurate libdevice exp/erfc/tanh, no fast-math) except where FP32 rounding
+// would dominate: the bond-order power takes a double-float exponent
+// (powf_dd.cuh) and the RI exponentials double-float arguments.  Tersoff site
+// energies and virials are summed per atom in FP32 and across atoms in FP64,
+// pair-potential sums per atom in compensated FP32 and then FP64; the loss and
 // normalisers are FP64.
 //
-// Geometry (unit vectors, distances, reverse-bond positions, RI Coulomb terms)
-// is parameter-independent and precomputed once (geometry.cu); three-body
-// cosines are dot products of the FP32 unit vectors, formed in registers.
+// Geometry (unit vectors, distances, reverse-bond positions, RI Coulomb terms
+// and type-grouped RI pair copies) is parameter-independent and precomputed
+// once (geometry.cu); three-body cosines are dot products of the FP32 unit
+// vectors, formed in registers.
 #include <algorithm>
 #include <cmath>
 #include <tuple>
