@@ -31,7 +31,8 @@ class GpugaError(RuntimeError):
 
 class Options(C.Structure):
     _fields_ = [("device", C.c_int), ("path", C.c_int), ("use_graph", C.c_int), ("nn2b_consistent", C.c_int),
-                ("nn2b_r1", C.c_float), ("nn2b_r2", C.c_float), ("verbose", C.c_int), ("neighbor_cells", C.c_int)]
+                ("nn2b_r1", C.c_float), ("nn2b_r2", C.c_float), ("verbose", C.c_int), ("neighbor_cells", C.c_int),
+                ("ri_self_energy", C.c_int)]
 
 
 FITNESS_CB = C.CFUNCTYPE(None, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_void_p)

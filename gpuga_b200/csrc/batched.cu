@@ -44,13 +44,15 @@ enum { TC_LR = 0, TC_LA = 2, TC_CR = 4, TC_CA = 6, TC_R0 = 8, TC_EN = 10, TC_BET
        TC_MHON, TC_COUNT };
 // RI (ri.cu:36-110): qq[3], a[3], b[3] = 1/rho, c[3], rc, v_rc, dv_rc, Morse lr, la, cr, ca, r0,
 // then the FP64 remainders of b[3], lr and la (their FP32 roundings would otherwise shift the
-// exponents |d/rho|, |lr (d - r0)| of up to ~20 by 2^-24 relative).
+// exponents |d/rho|, |lr (d - r0)| of up to ~20 by 2^-24 relative), and the self-energy
+// coefficient K_C q^2 S(rc) as an FP32 pair (hi, lo) so that the energy items rebuild it in FP64.
 enum { RC_QQ = 0, RC_A = 3, RC_B = 6, RC_C = 9, RC_RC = 12, RC_VRC, RC_DVRC, RC_LR, RC_LA, RC_CR, RC_CA, RC_R0,
-       RC_BLO, RC_LRLO = RC_BLO + 3, RC_LALO, RC_COUNT };
+       RC_BLO, RC_LRLO = RC_BLO + 3, RC_LALO, RC_SELF, RC_SELFLO, RC_COUNT };
+static_assert(RC_COUNT <= kMaxConsts, "per-individual RI constants");
 
 int consts_per_individual(const DevSet& d) {
   if (d.potential_type == 1 || d.potential_type == 2) return TC_COUNT;
-  if (d.potential_type == 0) return RC_COUNT;
+  if (is_ri_type(d.potential_type)) return RC_COUNT;
   return 1;
 }
 
@@ -94,12 +96,12 @@ __global__ void decode_jobs(const JobView* __restrict__ jobs, const int2* __rest
     put(TC_R2, R2);
     put(TC_PF, M_PI / (R2 - R1));
     put(TC_MHON, -0.5 / en);
-  } else if (potential_type == 0) {
-    const double q0 = par(0);
+  } else if (is_ri_type(potential_type)) {
+    const double q0 = par(0), ratio = ri_charge_ratio(potential_type);
     const double kc = 14.399645;  // ri.cu:29
     put(RC_QQ + 0, q0 * q0 * kc);
-    put(RC_QQ + 1, -0.5 * q0 * q0 * kc);
-    put(RC_QQ + 2, 0.25 * q0 * q0 * kc);
+    put(RC_QQ + 1, ratio * q0 * q0 * kc);
+    put(RC_QQ + 2, ratio * ratio * q0 * q0 * kc);
     for (int t = 0; t < 3; ++t) {
       put(RC_A + t, par(1 + 3 * t));
       put(RC_B + t, 1.0 / par(2 + 3 * t));
@@ -120,6 +122,13 @@ __global__ void decode_jobs(const JobView* __restrict__ jobs, const int2* __rest
     put(RC_CR, d0 / (s - 1.0));
     put(RC_CA, s * d0 / (s - 1.0));
     put(RC_R0, r0);
+    // damped-Coulomb self energy per unit (q_i / q)^2 (develop/hfo2/find_E.m:10-13)
+    const double self = J.ri_self ? q0 * q0 * kc *
+                                        (alpha / sqrt(M_PI) + erfc(alpha * rc) / rc +
+                                         0.5 * pif * exp(-alpha * alpha * rc * rc))
+                                  : 0.0;
+    put(RC_SELF, self);
+    put_lo(RC_SELFLO, self);
   } else {
     for (int m = 0; m < nv; ++m) weights[(size_t)m * Pstride + p] = decode1(pmin[m], pmax[m], x[m]);
   }
@@ -670,6 +679,15 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
   const Consts kc{J.consts, Pstride, pl};
   RIC R;
   if (KIND == 1) load_ri(kc, R);
+  const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
+  const int N = S.N;
+  double acc[kResK];
+#pragma unroll
+  for (int k = 0; k < kResK; ++k) acc[k] = 0.0;
+  // RI self energy: an energy item covers all atoms of its configuration, so warp 0 adds
+  // -K_C q^2 S sum_i (q_i / q)^2 once per individual, in FP64
+  if (KIND == 1 && !FORCE && J.ri_self && warp == 0)
+    acc[0] = -((double)kc[RC_SELF] + (double)kc[RC_SELFLO]) * S.ri_qsum[c];
   float* wsm = reinterpret_cast<float*>(smem + (size_t)kWarps * 32 * kResK * sizeof(double));
   if (KIND == 2) {
     for (size_t t = threadIdx.x; t < NNSmem<NMAX>::floats; t += blockDim.x) wsm[t] = 0.f;  // zero padding
@@ -681,11 +699,6 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
     }
     __syncthreads();
   }
-  const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
-  const int N = S.N;
-  double acc[kResK];
-#pragma unroll
-  for (int k = 0; k < kResK; ++k) acc[k] = 0.0;
   // per-atom sums over the atom's pairs: compensated FP32 (Kahan), added to the
   // FP64 accumulators once per atom -- a per-pair FP64 add would cost two
   // FP32->FP64 conversions per term, which run at a fraction of the FP32 rate
@@ -930,6 +943,7 @@ DevView make_view(const DevSet& d) {
   v.rgri = d.rgri;
   v.rseg = d.rseg;
   v.force_ref = d.force_ref;
+  v.ri_qsum = d.ri_qsum;
   return v;
 }
 
@@ -945,6 +959,7 @@ JobView make_job_view(const Engine* e, const Plan* plan) {
   j.Pstride = plan->Pstride;
   j.Nc_force = d.Nc_force;
   j.ri_fixed_rc = d.ri_fixed_rc;
+  j.ri_self = e->spec.ri_self;
   j.tp = NNTaper{e->spec.nn_r1, e->spec.nn_r2, (float)(M_PI / ((double)e->spec.nn_r2 - e->spec.nn_r1)),
                  e->spec.nn_consistent};
   j.pop = plan->d_pop;
@@ -1011,7 +1026,7 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
   const DevSet& d = e->d;
   const TrainingSet& ts = e->ts;
   const bool tersoff = d.potential_type == 1 || d.potential_type == 2;
-  const int kind = tersoff ? 0 : (d.potential_type == 0 ? 1 : 2);
+  const int kind = tersoff ? 0 : (is_ri_type(d.potential_type) ? 1 : 2);
   // NN2B: register-array size of the MLP; Tersoff: number of atom types (kernel template)
   const int nmax = kind == 2 ? nmax_of(d.num_neurons) : (kind == 0 ? d.num_types : 0);
   if (kind == 2 && nmax == 0) {

@@ -61,6 +61,7 @@ static int finish_create(PotentialSpec& spec, TrainingSet&& ts, const gpuga_opti
   spec.nn_r1 = o.nn2b_r1;
   spec.nn_r2 = o.nn2b_r2;
   spec.nn_consistent = o.nn2b_consistent;
+  spec.ri_self = o.ri_self_energy ? 1 : 0;
   if (spec.type == 3 && !(spec.nn_r2 > spec.nn_r1)) {
     set_error("NN2B taper needs r2 > r1 (got %g, %g).", spec.nn_r1, spec.nn_r2);
     return GPUGA_ERR_ARG;

@@ -32,7 +32,8 @@ int cuda_status(cudaError_t e, const char* what, const char* file, int line);
 
 // potential.in (fitness.cu:220-314) plus the engine's NN2B options.
 struct PotentialSpec {
-  int type = -1;         // 0 RI, 1 Tersoff one-element, 2 Tersoff two-element, 3 NN2B
+  int type = -1;         // 0 RI, 1 Tersoff one-element, 2 Tersoff two-element, 3 NN2B,
+                         // 4 RI with anion charge -q (charge-neutral 1:1 lattices; extension)
   int num_neurons = 0;   // NN2B only
   int num_vars = 0;
   float cutoff = 0.f;    // neighbor-list cutoff
@@ -40,7 +41,13 @@ struct PotentialSpec {
   std::vector<float> pmin, pmax;
   float nn_r1 = 7.0f, nn_r2 = 8.0f;  // nn2b.cuh:36-37
   int nn_consistent = 0;              // 0 keeps nn2b.cu:147-148 order
+  int ri_self = 0;                    // RI: subtract the damped-Coulomb self energy (off in ri.cu)
 };
+
+// RI and its charge-neutral variant share every kernel; only the anion charge differs.
+__host__ __device__ inline bool is_ri_type(int t) { return t == 0 || t == 4; }
+// anion charge / cation charge: -1/2 in ri.cu:40-43, -1 for potential type 4
+__host__ __device__ inline double ri_charge_ratio(int t) { return t == 4 ? -1.0 : -0.5; }
 
 // train.in after parsing (fitness.cu:59-182), in the reference's layouts.
 struct TrainingSet {

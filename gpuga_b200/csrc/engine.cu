@@ -69,12 +69,17 @@ int engine_create(const PotentialSpec& spec, TrainingSet&& ts, const gpuga_optio
   d.w_force = spec.w_force;
   d.w_energy = spec.w_energy;
   d.w_stress = spec.w_stress;
-  if (spec.type == 0) {
+  if (is_ri_type(spec.type)) {
     for (int v : t.type)
       if (v < 0 || v > 1) {
         set_error("the RI potential expects atom types 0 (cation) and 1 (anion); found %d.", v);
         return GPUGA_ERR_PARSE;
       }
+    const double r2 = ri_charge_ratio(spec.type) * ri_charge_ratio(spec.type);
+    std::vector<double> qsum(t.Nc, 0.0);
+    for (int c = 0; c < t.Nc; ++c)
+      for (int k = 0; k < t.Na[c]; ++k) qsum[c] += t.type[t.Na_sum[c] + k] == 0 ? 1.0 : r2;
+    GPUGA_TRY(upload(e.get(), &d.ri_qsum, qsum.data(), qsum.size()));
   }
   if (spec.type == 2) {
     for (int v : t.type)

@@ -65,6 +65,8 @@ struct DevSet {
   // RI: the Coulomb shift cutoff (parameter 10) is the same for every individual, so the
   // shifted, damped Coulomb term is precomputed per bond in FP64 (gri.z, gri.w)
   int ri_fixed_rc = 0;
+  // RI: per configuration sum_i (q_i / q)^2 = cations + ratio^2 anions (the self-energy weight)
+  double* ri_qsum = nullptr;
 };
 
 // One CTA of a batched launch: configuration `config` of job `job` for
@@ -93,6 +95,7 @@ struct DevView {
   const float4* rgri;
   const int4* rseg;
   const float* force_ref;
+  const double* ri_qsum;
 };
 
 struct NNTaper {
@@ -104,7 +107,7 @@ struct NNTaper {
 // buffers of its evaluation.  Several jobs share the same launches.
 struct JobView {
   DevView v;
-  int potential_type, num_types, num_neurons, num_vars, P, Pstride, Nc_force, ri_fixed_rc;
+  int potential_type, num_types, num_neurons, num_vars, P, Pstride, Nc_force, ri_fixed_rc, ri_self;
   NNTaper tp;
   const float* pop;      // [P][num_vars] in [0,1]
   const float* pmin;

@@ -517,7 +517,7 @@ int build_geometry(Engine* e) {
 
   GPUGA_TRY(e->alloc(&d.g64, std::max(B, 1)));
   // RI evaluates its type-grouped copies (rg32 / rgri, below): there g32 and gri are scratch
-  const bool ri = d.potential_type == 0;
+  const bool ri = is_ri_type(d.potential_type);
   if (ri) {
     GPUGA_CUDA(cudaMalloc(&d.g32, sizeof(float4) * std::max(B, 1)));
     GPUGA_CUDA(cudaMalloc(&d.gri, sizeof(float4) * std::max(B, 1)));
@@ -528,19 +528,19 @@ int build_geometry(Engine* e) {
   GPUGA_TRY(e->alloc(&d.half_off, N));
   GPUGA_TRY(e->alloc(&d.ptype, std::max(B, 1)));
   double rc_fixed = 0.0;
-  if (d.potential_type == 0 && e->spec.pmin.size() > 10 && e->spec.pmin[10] == e->spec.pmax[10] &&
+  if (ri && e->spec.pmin.size() > 10 && e->spec.pmin[10] == e->spec.pmax[10] &&
       e->spec.pmin[10] > 0) {
     rc_fixed = e->spec.pmin[10];
     d.ri_fixed_rc = 1;
   }
   bond_geometry<<<(N + 127) / 128, 128, 0, st>>>(N, d_atom_cfg, d.h, d.r, d.type, d.off, d.nbr, img,
-                                                 d.potential_type, d.num_types, rc_fixed, d.g64, d.g32, d.gri, d.rev,
+                                                 ri ? 0 : d.potential_type, d.num_types, rc_fixed, d.g64, d.g32, d.gri, d.rev,
                                                  d.half_off, d.ptype);
   GPUGA_CUDA(cudaGetLastError());
   GPUGA_TRY(e->alloc(&d.rev_sm, std::max(B, 1)));
   reverse_slots<<<(N + 127) / 128, 128, 0, st>>>(N, d_atom_cfg, d.Na, d.Na_sum, d.off, d.nbr, d.rev, d.rev_sm);
   GPUGA_CUDA(cudaGetLastError());
-  if (d.potential_type == 0) {
+  if (ri) {
     std::vector<int> half(N), start(N + 1, 0);
     GPUGA_CUDA(cudaMemcpyAsync(half.data(), d.half_off, sizeof(int) * N, cudaMemcpyDeviceToHost, st));
     GPUGA_CUDA(cudaStreamSynchronize(st));

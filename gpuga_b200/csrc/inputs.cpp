@@ -53,6 +53,7 @@ int num_vars_for(int potential_type, int num_neurons) {
     case 1: return 9;   // fitness.cu:241-244
     case 2: return 13;  // fitness.cu:245-248
     case 3: return num_neurons * (num_neurons + 4) + 1;  // fitness.cu:249-258
+    case 4: return 15;  // RI parameters, anion charge -q
     default: return -1;
   }
 }
@@ -100,7 +101,7 @@ int read_potential_in(const std::string& dir, PotentialSpec* spec) {
     }
   }
   for (int n = 0; n < spec->num_vars; ++n) {
-    if (spec->type < 3) {
+    if (spec->type != 3) {
       if (fscanf(f.get(), "%255s%f%f", name, &spec->pmin[n], &spec->pmax[n]) != 3) {
         set_error("reading error for potential.in.");
         return GPUGA_ERR_PARSE;

@@ -14,9 +14,15 @@ struct PT {  // minimal Tersoff constants
   T D0[2], A[2], R0[2], S[2], EN, BETA, H, R1, R2, PF, MHON;
 };
 template <class T>
-struct PR {  // RI constants (ri.cu:21-25)
-  T a[3], b[3], c[3], qq[3], v_rc, dv_rc, cutoff, d0, alpha, r0, s;
+struct PR {  // RI constants (ri.cu:21-25); self: K_C S(rc) of the optional self energy (0 when off)
+  T a[3], b[3], c[3], qq[3], v_rc, dv_rc, cutoff, d0, alpha, r0, s, self;
 };
+
+// Damped-Coulomb self energy per K_C q_i^2 (develop/hfo2/find_E.m:10-13).
+inline double ri_self_factor(double rc) {
+  const double alpha = 0.2, pif = 0.225675833419103;
+  return alpha / sqrt(M_PI) + erfc(alpha * rc) / rc + 0.5 * pif * exp(-alpha * alpha * rc * rc);
+}
 struct PN {
   int n;
   double r1, r2, pf;
@@ -300,6 +306,7 @@ __global__ void p_pair(int N, int kind, const int* __restrict__ type, Lay L, con
   W[n1 + 3 * (size_t)N] = vxy;
   W[n1 + 4 * (size_t)N] = vyz;
   W[n1 + 5 * (size_t)N] = vzx;
+  if (kind == 0) e -= q.qq[type[n1] == 0 ? 0 : 2] * q.self;
   pe[n1] = e;
 }
 
@@ -389,12 +396,13 @@ PT<T> tersoff_consts(const float* p, int num_types) {
 }
 
 template <class T>
-PR<T> ri_consts(const float* p) {
+PR<T> ri_consts(const float* p, int potential_type, bool with_self) {
   PR<T> r;
   const double q0 = p[0], kc = 14.399645, alpha = 0.2, pif = 0.225675833419103;
+  const double ratio = ri_charge_ratio(potential_type);
   r.qq[0] = (T)(q0 * q0 * kc);
-  r.qq[1] = (T)(-0.5 * q0 * q0 * kc);
-  r.qq[2] = (T)(0.25 * q0 * q0 * kc);
+  r.qq[1] = (T)(ratio * q0 * q0 * kc);
+  r.qq[2] = (T)(ratio * ratio * q0 * q0 * kc);
   for (int t = 0; t < 3; ++t) {
     r.a[t] = p[1 + 3 * t];
     r.b[t] = (T)(1.0 / (double)p[2 + 3 * t]);
@@ -408,6 +416,7 @@ PR<T> ri_consts(const float* p) {
   r.s = p[14];
   r.v_rc = (T)(erfc(alpha * rc) / rc);
   r.dv_rc = (T)(-erfc(alpha * rc) / (rc * rc) - pif * exp(-alpha * alpha * rc * rc) / rc);
+  r.self = with_self ? (T)ri_self_factor(rc) : T(0);
   return r;
 }
 
@@ -462,8 +471,8 @@ int enqueue_force(Engine* e, const float* params, const Scratch<T>& s, cudaStrea
     PR<T> q{};
     PN nn{d.num_neurons, e->spec.nn_r1, e->spec.nn_r2, M_PI / ((double)e->spec.nn_r2 - e->spec.nn_r1),
           e->spec.nn_consistent};
-    if (d.potential_type == 0) {
-      q = ri_consts<T>(params);
+    if (is_ri_type(d.potential_type)) {
+      q = ri_consts<T>(params, d.potential_type, e->spec.ri_self != 0);
     } else {
       if (d.num_neurons > 32) {
         set_error("the plain NN2B path supports up to 32 neurons per layer.");
@@ -474,7 +483,7 @@ int enqueue_force(Engine* e, const float* params, const Scratch<T>& s, cudaStrea
       GPUGA_CUDA(cudaMemcpyAsync(s.w, w.data(), sizeof(T) * d.num_vars, cudaMemcpyHostToDevice, st));
       GPUGA_CUDA(cudaStreamSynchronize(st));  // w is a stack buffer
     }
-    p_pair<T><<<grid, 128, 0, st>>>(N, d.potential_type == 0 ? 0 : 1, d.type, CsrLayout{d.off, d.nbr}, d.g64, q,
+    p_pair<T><<<grid, 128, 0, st>>>(N, is_ri_type(d.potential_type) ? 0 : 1, d.type, CsrLayout{d.off, d.nbr}, d.g64, q,
                                     s.w, nn, s.F, s.W, s.pe);
   }
   GPUGA_CUDA(cudaGetLastError());
@@ -556,11 +565,12 @@ int plain_find_force64(Engine* e, const double* params, double* F, double* W, do
     PR<double> q{};
     PN nn{d.num_neurons, e->spec.nn_r1, e->spec.nn_r2, M_PI / ((double)e->spec.nn_r2 - e->spec.nn_r1),
           e->spec.nn_consistent};
-    if (d.potential_type == 0) {
+    if (is_ri_type(d.potential_type)) {
       const double q0 = params[0], kc = 14.399645, alpha = 0.2, pif = 0.225675833419103;
+      const double ratio = ri_charge_ratio(d.potential_type);
       q.qq[0] = q0 * q0 * kc;
-      q.qq[1] = -0.5 * q0 * q0 * kc;
-      q.qq[2] = 0.25 * q0 * q0 * kc;
+      q.qq[1] = ratio * q0 * q0 * kc;
+      q.qq[2] = ratio * ratio * q0 * q0 * kc;
       for (int t = 0; t < 3; ++t) {
         q.a[t] = params[1 + 3 * t];
         q.b[t] = 1.0 / params[2 + 3 * t];
@@ -574,6 +584,7 @@ int plain_find_force64(Engine* e, const double* params, double* F, double* W, do
       q.v_rc = erfc(alpha * q.cutoff) / q.cutoff;
       q.dv_rc = -erfc(alpha * q.cutoff) / (q.cutoff * q.cutoff) -
                 pif * exp(-alpha * alpha * q.cutoff * q.cutoff) / q.cutoff;
+      q.self = e->spec.ri_self ? ri_self_factor(q.cutoff) : 0.0;
     } else {
       if (d.num_neurons > 32) {
         set_error("the plain NN2B path supports up to 32 neurons per layer.");
@@ -581,7 +592,7 @@ int plain_find_force64(Engine* e, const double* params, double* F, double* W, do
       }
       GPUGA_CUDA(cudaMemcpyAsync(s.w, params, sizeof(double) * d.num_vars, cudaMemcpyHostToDevice, st));
     }
-    p_pair<double><<<grid, 128, 0, st>>>(N, d.potential_type == 0 ? 0 : 1, d.type, CsrLayout{d.off, d.nbr}, d.g64,
+    p_pair<double><<<grid, 128, 0, st>>>(N, is_ri_type(d.potential_type) ? 0 : 1, d.type, CsrLayout{d.off, d.nbr}, d.g64,
                                          q, s.w, nn, s.F, s.W, s.pe);
   }
   GPUGA_CUDA(cudaGetLastError());
@@ -637,12 +648,12 @@ int ref_potential_find_force(int potential_type, int num_neurons, const float* p
     p_tersoff1<float><<<grid, 128, 0, st>>>(N, L, s.g64, P, b, bp);
     p_tersoff2<float><<<grid, 128, 0, st>>>(N, num_types, type, L, s.g64, P, b, bp, pe, fx, fy, fz);
     p_tersoff3<float><<<grid, 128, 0, st>>>(N, L, s.rev, s.g64, fx, fy, fz, f, virial);
-  } else if (potential_type == 0 || potential_type == 3) {
+  } else if (is_ri_type(potential_type) || potential_type == 3) {
     PR<float> q{};
     PN nn{num_neurons, nn_opts.nn_r1, nn_opts.nn_r2, M_PI / ((double)nn_opts.nn_r2 - nn_opts.nn_r1),
           nn_opts.nn_consistent};
-    if (potential_type == 0) {
-      q = ri_consts<float>(params);
+    if (is_ri_type(potential_type)) {
+      q = ri_consts<float>(params, potential_type, nn_opts.ri_self != 0);
     } else {
       if (num_neurons > 32) {
         set_error("the NN2B Potential entry points support up to 32 neurons per layer.");
@@ -651,7 +662,7 @@ int ref_potential_find_force(int potential_type, int num_neurons, const float* p
       GPUGA_CUDA(cudaMemcpyAsync(s.w, params, sizeof(float) * num_vars_for(3, num_neurons), cudaMemcpyHostToDevice,
                                  st));
     }
-    p_pair<float><<<grid, 128, 0, st>>>(N, potential_type == 0 ? 0 : 1, type, L, s.g64, q, s.w, nn, f, virial, pe);
+    p_pair<float><<<grid, 128, 0, st>>>(N, is_ri_type(potential_type) ? 0 : 1, type, L, s.g64, q, s.w, nn, f, virial, pe);
   } else {
     set_error("unsupported potential type %d.", potential_type);
     return GPUGA_ERR_UNSUPPORTED;

@@ -216,6 +216,7 @@ def write_dir(data: dict, path: str) -> str:
     names = {1: ["D0", "alpha", "r0", "S", "n", "beta", "h", "R1", "R2"],
              0: ["Q0", "A00", "rho00", "C00", "A01", "rho01", "C01", "A11", "rho11", "C11", "cutoff", "D0",
                  "alpha", "r0", "S"]}
+    names[4] = names[0]
     with open(os.path.join(path, "potential.in"), "w") as f:
         f.write(f"potential_type {pt}\n")
         if pt == 3:
@@ -223,7 +224,7 @@ def write_dir(data: dict, path: str) -> str:
         f.write(f"cutoff {float(data['cutoff']):.9g}\n")
         f.write(f"weight_force {float(data['w_force']):.9g}\nweight_energy {float(data['w_energy']):.9g}\n"
                 f"weight_virial {float(data['w_stress']):.9g}\n")
-        if pt < 3:
+        if pt != 3:
             for nm, lo, hi in zip(names.get(pt, [f"p{m}" for m in range(len(data['pmin']))]), data["pmin"],
                                   data["pmax"]):
                 f.write(f"{nm} {float(lo):.9g} {float(hi):.9g}\n")

@@ -31,6 +31,10 @@ extern "C" {
 #define GPUGA_ERR_CANCELLED (-10)  /* serving: job was cancelled */
 #define GPUGA_ERR_NOT_READY (-11)  /* serving: job still running */
 
+/* Potential types (potential.in, fitness.cu:220-258): 0 RI (cation +q, anion -q/2, ri.cu:40-43),
+ * 1 minimal Tersoff, 2 two-element minimal Tersoff, 3 NN2B, and 4 RI with anion charge -q
+ * (charge-neutral 1:1 lattices; no counterpart in the reference, which hard-codes -q/2). */
+
 /* Evaluation paths. */
 #define GPUGA_PATH_BATCHED 0 /* all individuals x all configs per generation, FP32 math + FP64 sums */
 #define GPUGA_PATH_PLAIN64 1 /* one individual per launch, FP64 throughout */
@@ -52,6 +56,9 @@ typedef struct gpuga_options {
   int neighbor_cells;  /* neighbor build: 0 cell lists for configurations of >= 2048 atoms (default),
                           1 cell lists wherever the box holds >= 3 cells of width rc per direction,
                           2 the O(Na^2) scan of neighbor.cu:30-66 everywhere; the lists are identical */
+  int ri_self_energy;  /* RI (potential types 0 and 4): 1 subtracts the damped-Coulomb self energy
+                          -K_C sum_i q_i^2 [alpha/sqrt(pi) + erfc(alpha rc)/rc + alpha/sqrt(pi) exp(-alpha^2 rc^2)]
+                          from every atom's energy, in FP64; 0 (default) keeps ri.cu, which has none */
 } gpuga_options;
 
 /* Fills *opt with the reference's semantics (batched path, graphs on, NN2B taper 7..8 A, force quirk kept). */

@@ -35,7 +35,8 @@ namespace {
 
 struct OSet {
   // potential.in
-  int potential_type = -1;
+  int potential_type = -1;  // 0 RI, 1/2 Tersoff, 3 NN2B, 4 RI with anion charge -q (extension)
+  int ri_self = 0;          // RI: subtract the damped-Coulomb self energy (opt-in extension)
   int num_neurons = 0;
   int num_vars = 0;
   float cutoff = 0.f;
@@ -71,7 +72,8 @@ bool read_potential(OSet* s, const char* dir) {
   char name[256];
   if (fscanf(f, "%255s%d", name, &s->potential_type) != 2) { fclose(f); return fail(s, "potential.in: type"); }
   switch (s->potential_type) {
-    case 0: s->num_vars = 15; break;
+    case 0:
+    case 4: s->num_vars = 15; break;
     case 1: s->num_vars = 9; break;
     case 2: s->num_vars = 13; break;
     case 3:
@@ -87,7 +89,7 @@ bool read_potential(OSet* s, const char* dir) {
   if (fscanf(f, "%255s%f", name, &s->w_energy) != 2 || s->w_energy < 0) { fclose(f); return fail(s, "potential.in: weight_energy"); }
   if (fscanf(f, "%255s%f", name, &s->w_stress) != 2 || s->w_stress < 0) { fclose(f); return fail(s, "potential.in: weight_stress"); }
   for (int n = 0; n < s->num_vars; ++n) {
-    if (s->potential_type < 3) {
+    if (s->potential_type != 3) {
       if (fscanf(f, "%255s%f%f", name, &s->pmin[n], &s->pmax[n]) != 3) { fclose(f); return fail(s, "potential.in: bounds"); }
     } else {
       s->pmin[n] = -3.0f;
@@ -427,16 +429,20 @@ void tersoff_force(const OSet* s, const double* p, double* F, double* W, double*
 
 // ri.cu:26-29 constants, ri.cu:36-74 parameter set-up
 struct RIP {
-  double a[3], b[3], c[3], qq[3], v_rc, dv_rc, cutoff, d0, alpha, r0, s;
+  double a[3], b[3], c[3], qq[3], v_rc, dv_rc, cutoff, d0, alpha, r0, s, self;
 };
 const double RI_ALPHA = 0.2, RI_ALPHA_SQ = 0.04, RI_PIF = 0.225675833419103, RI_KC = 14.399645;
 
-RIP ri_params(const double* p) {
+// Charges: cation +q, anion -q/2 (ri.cu:40-43) for potential_type 0; anion -q for the neutral
+// variant 4.  self: the damped-Coulomb self-energy factor of develop/hfo2/find_E.m:10-13 (the
+// teacher there multiplies it by 0): E_self = -K_C sum_i q_i^2 self.
+RIP ri_params(const double* p, int potential_type, bool with_self) {
   RIP r;
   const double q0 = p[0];
+  const double ratio = potential_type == 4 ? -1.0 : -0.5;
   r.qq[0] = q0 * q0 * RI_KC;
-  r.qq[1] = -0.5 * q0 * q0 * RI_KC;
-  r.qq[2] = 0.25 * q0 * q0 * RI_KC;
+  r.qq[1] = ratio * q0 * q0 * RI_KC;
+  r.qq[2] = ratio * ratio * q0 * q0 * RI_KC;
   for (int t = 0; t < 3; ++t) {
     r.a[t] = p[1 + 3 * t];
     r.b[t] = 1.0 / p[2 + 3 * t];
@@ -447,6 +453,10 @@ RIP ri_params(const double* p) {
   r.v_rc = std::erfc(RI_ALPHA * r.cutoff) / r.cutoff;
   r.dv_rc = -std::erfc(RI_ALPHA * r.cutoff) / (r.cutoff * r.cutoff);
   r.dv_rc -= RI_PIF * std::exp(-RI_ALPHA_SQ * r.cutoff * r.cutoff) / r.cutoff;
+  const double rc = r.cutoff, erfc_rc = std::erfc(RI_ALPHA * rc);
+  r.self = with_self ? RI_ALPHA / std::sqrt(M_PI) + 0.5 * erfc_rc / rc +
+                           0.5 * (erfc_rc / rc + RI_PIF * std::exp(-RI_ALPHA_SQ * rc * rc))
+                     : 0.0;
   return r;
 }
 
@@ -497,9 +507,9 @@ inline void nn_p2_f2(const double* p, int n, double d, double& p2, double& f2) {
 // ri.cu:112-189 and nn2b.cu:94-173: owner-computes pair loop over the full list
 void pair_force(const OSet* s, const double* p, double* F, double* W, double* pe) {
   const int N = s->N;
-  const bool is_ri = s->potential_type == 0;
+  const bool is_ri = s->potential_type == 0 || s->potential_type == 4;
   RIP q;
-  if (is_ri) q = ri_params(p);
+  if (is_ri) q = ri_params(p, s->potential_type, s->ri_self != 0);
   const int n = s->num_neurons;
   const double pf = M_PI / (s->nn_r2 - s->nn_r1);
 #pragma omp parallel for schedule(static)
@@ -535,6 +545,7 @@ void pair_force(const OSet* s, const double* p, double* F, double* W, double* pe
     F[n1] = fx; F[n1 + N] = fy; F[n1 + 2 * N] = fz;
     W[n1] = vxx; W[n1 + N] = vyy; W[n1 + 2 * N] = vzz;
     W[n1 + 3 * N] = vxy; W[n1 + 4 * N] = vyz; W[n1 + 5 * N] = vzx;
+    if (is_ri) e -= (s->type[n1] == 0 ? q.qq[0] : q.qq[2]) * q.self;
     pe[n1] = e;
   }
 }
@@ -641,6 +652,8 @@ void oracle_neighbors(void* h, int* NN, int* nl) {
   std::copy(s->NN.begin(), s->NN.end(), NN);
   std::copy(s->nl.begin(), s->nl.end(), nl);
 }
+
+void oracle_set_ri_self(void* h, int on) { static_cast<OSet*>(h)->ri_self = on; }
 
 void oracle_set_nn2b(void* h, double r1, double r2, int consistent) {
   OSet* s = (OSet*)h;

@@ -37,6 +37,7 @@ def lib():
         L.oracle_arrays.argtypes = [C.c_void_p] + [C.c_void_p] * 8
         L.oracle_neighbors.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_set_nn2b.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
+        L.oracle_set_ri_self.argtypes = [C.c_void_p, C.c_int]
         L.oracle_decode.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_find_force.argtypes = [C.c_void_p] + [C.c_void_p] * 4
         L.oracle_config_sums.argtypes = [C.c_void_p] + [C.c_void_p] * 4
@@ -110,6 +111,10 @@ class OracleSet:
 
     def set_nn2b(self, r1: float = 7.0, r2: float = 8.0, consistent: bool = False):
         lib().oracle_set_nn2b(self._h, r1, r2, int(consistent))
+
+    def set_ri_self(self, on: bool) -> None:
+        """RI: subtract the damped-Coulomb self energy (develop/hfo2/find_E.m:10-13)."""
+        lib().oracle_set_ri_self(self._h, int(on))
 
     def decode(self, x01) -> np.ndarray:
         x = np.ascontiguousarray(x01, np.float32)

@@ -35,6 +35,8 @@ def oracle_targets(oracle_mod):
         s = oracle_mod.OracleSet(d)
         if int(data["potential_type"]) == 3:
             s.set_nn2b(data.get("nn2b_r1", 7.0), data.get("nn2b_r2", 8.0), False)
+        if data.get("ri_self_energy"):
+            s.set_ri_self(True)
         return s.find_force(params)
     return evaluate
 
