@@ -269,10 +269,13 @@ __device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int N
 // the reference's f_ij (minimal_tersoff.cu:250-307) is
 //   f_ij = 1/2 [ (A'_j - fc'_j sum_k T_k g_jk - m_j sum_k q_jk cos_jk) u_j + m_j sum_k q_jk u_k ]
 // with q_jk = beta (cos_jk - h) (S_j fc_k + T_k) and m_j = -2 fc_j / d_j.
-template <int ZC, int NT, bool FORCE>
+//
+// FULL: every one of the ZC bond slots is present (Z == ZC, e.g. all atoms of a diamond
+// lattice), so that the per-slot guards fold away at compile time.
+template <int ZC, int NT, bool FORCE, bool FULL>
 __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C, int il, int Na, float* fsm, int G,
                                               int g, float (&v)[6]) {
-  const int Z = geo.nn[il];
+  const int Z = FULL ? ZC : geo.nn[il];
   const int b0 = geo.base(il), bs = geo.step();  // bond j at b0 + j * bs
   float ux[ZC], uy[ZC], uz[ZC], dd[ZC];
   int st[ZC];
@@ -437,9 +440,12 @@ __global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_ba
                       : Geo{S.g32 + bond0, S.ptype + bond0, S.rev_sm + bond0, S.NN + atom0, S.off + atom0, bond0, 0};
   for (int base = warp * A; base < Na; base += NW * A) {
     const int il = base + aslot;
+    // warp-uniform choice of the guard-free form (no divergence between the two)
+    const bool full = __all_sync(0xffffffffu, il >= Na || geo.nn[il] == ZC);
     if (il < Na) {
       float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      const float pe = tersoff_atom<ZC, NT, FORCE>(geo, C, il, Na, fsm, G, g, v);
+      const float pe = full ? tersoff_atom<ZC, NT, FORCE, true>(geo, C, il, Na, fsm, G, g, v)
+                            : tersoff_atom<ZC, NT, FORCE, false>(geo, C, il, Na, fsm, G, g, v);
       if (!FORCE) {
         red[threadIdx.x] += (double)pe;
 #pragma unroll
