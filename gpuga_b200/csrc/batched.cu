@@ -194,19 +194,22 @@ __host__ __device__ __forceinline__ int pack_G(int G, bool staged, size_t fbytes
 }
 
 // Fixed-order fold of per-lane partial sums held in shared memory as
-// red[k * blockDim.x + thread] into res[p][c][k]: lanes of the same individual
-// (one per warp and atom slot) are added in thread order.
+// red[k * blockDim.x + thread] into res[p][c][k], one warp per k: lane l first adds
+// the partials of lane l of every warp (warp order), then a butterfly over the lanes
+// of the same individual (l mod G) adds across atom slots.  Both partners of a
+// butterfly step form the same sum, so the result is deterministic, and every chain is
+// short (a sequential fold over 32/G atom slots per warp stalled the CTA).
 __device__ __forceinline__ void fold_item(const WorkItem& it, int P, int Nc, const double* red,
                                           double* __restrict__ res) {
   __syncthreads();
-  const int G = item_G(it), A = 32 / G, nw = blockDim.x >> 5;
-  for (int t = threadIdx.x; t < G * kResK; t += blockDim.x) {
-    const int gg = t % G, k = t / G;
+  const int G = item_G(it), nw = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31;
+  for (int k = threadIdx.x >> 5; k < kResK; k += nw) {
     double s = 0.0;
-    for (int w = 0; w < nw; ++w)
-      for (int a = 0; a < A; ++a) s += red[(size_t)k * blockDim.x + w * 32 + a * G + gg];
-    const int p = it.p0 + gg;
-    if (p < P) res[((size_t)p * Nc + it.config) * kResK + k] = s;
+    for (int w = 0; w < nw; ++w) s += red[(size_t)k * blockDim.x + w * 32 + lane];
+    for (int o = G; o < 32; o <<= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const int p = it.p0 + lane;
+    if (lane < G && p < P) res[((size_t)p * Nc + it.config) * kResK + k] = s;
   }
 }
 
@@ -467,11 +470,17 @@ __global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_ba
       const int i = atom0 + il;
       const int b0 = geo.base(il), bs = geo.step(), Z = geo.nn[il];
       float Fx = 0.f, Fy = 0.f, Fz = 0.f;
-      for (int j = 0; j < Z; ++j) {
-        const int bl = j * Na + il, rl = geo.rev[b0 + j * bs];
-        Fx += fsm[(bl * 3 + 0) * G + g] - fsm[(rl * 3 + 0) * G + g];
-        Fy += fsm[(bl * 3 + 1) * G + g] - fsm[(rl * 3 + 1) * G + g];
-        Fz += fsm[(bl * 3 + 2) * G + g] - fsm[(rl * 3 + 2) * G + g];
+      int rls[ZC];
+#pragma unroll
+      for (int j = 0; j < ZC; ++j) rls[j] = j < Z ? geo.rev[b0 + j * bs] : 0;
+#pragma unroll
+      for (int j = 0; j < ZC; ++j) {
+        if (j < Z) {
+          const int bl = j * Na + il, rl = rls[j];
+          Fx += fsm[(bl * 3 + 0) * G + g] - fsm[(rl * 3 + 0) * G + g];
+          Fy += fsm[(bl * 3 + 1) * G + g] - fsm[(rl * 3 + 1) * G + g];
+          Fz += fsm[(bl * 3 + 2) * G + g] - fsm[(rl * 3 + 2) * G + g];
+        }
       }
       const double dx = (double)Fx - (double)S.force_ref[i];
       const double dy = (double)Fy - (double)S.force_ref[i + N];
