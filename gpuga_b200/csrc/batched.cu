@@ -409,19 +409,19 @@ __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C,
 // memory (red[k][thread]) to save registers; a staged item's geometry follows
 // that region.  Force items put the f_ij scratch first, the staged geometry
 // after it, and reuse the start of shared memory for the final fold.
-template <int ZC, int NT, bool FORCE, int BLK>
-__global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_batched(const JobView* __restrict__ jobs,
-                                                       const WorkItem* __restrict__ items) {
-  extern __shared__ __align__(16) unsigned char smem[];
+// GT: the item's individuals per item G as a compile-time constant (0: read from the item), so
+// that the force scratch addressing and the atom-slot split fold into shifts and constants.
+template <int ZC, int NT, bool FORCE, int BLK, int GT>
+__device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, const WorkItem& it,
+                                             unsigned char* smem) {
   constexpr int NW = BLK / 32;
-  const WorkItem it = items[blockIdx.x];
   const JobView& J = jobs[it.job];
   const DevView S = J.v;
   const int P = J.P;
   double* __restrict__ res = J.res;
   float* __restrict__ fdump = J.fdump;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int G = item_G(it), A = 32 / G;
+  const int G = GT ? GT : item_G(it), A = 32 / G;
   const int g = lane & (G - 1), aslot = lane / G;
   const int p = it.p0 + g;
   const Consts kc{J.consts, J.Pstride, p < P ? p : it.p0};
@@ -498,6 +498,27 @@ __global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_ba
   for (int k = 0; k < 7; ++k) red[k * BLK + threadIdx.x] = 0.0;
   red[7 * BLK + threadIdx.x] = ferr;
   fold_item(it, P, S.Nc, red, res);
+}
+
+template <int ZC, int NT, bool FORCE, int BLK>
+__global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_batched(const JobView* __restrict__ jobs,
+                                                       const WorkItem* __restrict__ items) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const WorkItem it = items[blockIdx.x];
+  if constexpr (!FORCE) {
+    tersoff_item<ZC, NT, FORCE, BLK, 32>(jobs, it, smem);  // energy/virial items: always 32 individuals
+  } else if constexpr (ZC == 4) {
+    switch (item_G(it)) {
+      case 32: tersoff_item<ZC, NT, FORCE, BLK, 32>(jobs, it, smem); break;
+      case 16: tersoff_item<ZC, NT, FORCE, BLK, 16>(jobs, it, smem); break;
+      case 8: tersoff_item<ZC, NT, FORCE, BLK, 8>(jobs, it, smem); break;
+      case 4: tersoff_item<ZC, NT, FORCE, BLK, 4>(jobs, it, smem); break;
+      case 2: tersoff_item<ZC, NT, FORCE, BLK, 2>(jobs, it, smem); break;
+      default: tersoff_item<ZC, NT, FORCE, BLK, 1>(jobs, it, smem); break;
+    }
+  } else {
+    tersoff_item<ZC, NT, FORCE, BLK, 0>(jobs, it, smem);
+  }
 }
 
 // --------------------------------------------------------------------------- RI / NN2B
@@ -1101,7 +1122,8 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
         fbytes = (per_ind * G + 15) & ~(size_t)15;
         smem = std::max(smem, fbytes + (staged ? stage : 0));
       } else {
-        // energy/virial items: per-lane FP64 sums of the 128-thread CTA, then (optionally) the geometry
+        // energy/virial items (always G = 32, which tersoff_batched compiles in): per-lane FP64
+        // sums of the 128-thread CTA, then (optionally) the geometry
         smem = (size_t)kBlockEV * kResK * sizeof(double);
         if (kStageEV && stage <= stage_target(zc)) {
           staged = true;
