@@ -228,7 +228,9 @@ __device__ __forceinline__ void reduce_item(const WorkItem& it, int P, int Nc, d
 // il at boff[il] - bond0 + j).  Staged: a slot-major copy in shared memory
 // (bond j of atom il at j * Na + il, `stride` = Na), so that the lanes of a warp,
 // which hold consecutive atoms, read consecutive entries without bank conflicts.
-struct Geo {
+// ST: 1 staged, 0 CSR, -1 decided at run time by `stride`.
+template <int ST>
+struct GeoT {
   const float4* g;     // (unit vector, d)
   const uint8_t* pt;   // pair set
   const int* rev;      // slot * Na + atom of the reverse bond (force scratch position)
@@ -236,9 +238,18 @@ struct Geo {
   const int* boff;     // [Na] bond offset (global numbering; subtract bond0), unstaged only
   int bond0;
   int stride;          // Na when staged (slot-major), 0 for the CSR arrays
-  __device__ __forceinline__ int base(int il) const { return stride ? il : boff[il] - bond0; }
-  __device__ __forceinline__ int step() const { return stride ? stride : 1; }
+  __device__ __forceinline__ int base(int il) const {
+    if constexpr (ST == 1) return il;
+    else if constexpr (ST == 0) return boff[il] - bond0;
+    else return stride ? il : boff[il] - bond0;
+  }
+  __device__ __forceinline__ int step() const {
+    if constexpr (ST == 1) return stride;
+    else if constexpr (ST == 0) return 1;
+    else return stride ? stride : 1;
+  }
 };
+using Geo = GeoT<-1>;
 
 // Copies configuration c's geometry into shared memory, slot-major with ZC
 // slots, with all threads of the CTA (independent loads, then one barrier).
@@ -275,8 +286,8 @@ __device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int N
 //
 // FULL: every one of the ZC bond slots is present (Z == ZC, e.g. all atoms of a diamond
 // lattice), so that the per-slot guards fold away at compile time.
-template <int ZC, int NT, bool FORCE, bool FULL>
-__device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C, int il, int Na, float* fsm, int G,
+template <int ZC, int NT, bool FORCE, bool FULL, class GEO>
+__device__ __forceinline__ float tersoff_atom(const GEO& geo, const TersoffC& C, int il, int Na, float* fsm, int G,
                                               int g, float (&v)[6]) {
   const int Z = FULL ? ZC : geo.nn[il];
   const int b0 = geo.base(il), bs = geo.step();  // bond j at b0 + j * bs
@@ -410,8 +421,9 @@ __device__ __forceinline__ float tersoff_atom(const Geo& geo, const TersoffC& C,
 // that region.  Force items put the f_ij scratch first, the staged geometry
 // after it, and reuse the start of shared memory for the final fold.
 // GT: the item's individuals per item G as a compile-time constant (0: read from the item), so
-// that the force scratch addressing and the atom-slot split fold into shifts and constants.
-template <int ZC, int NT, bool FORCE, int BLK, int GT>
+// that the force scratch addressing and the atom-slot split fold into shifts and constants;
+// ST: staged (1) or in-place CSR (0) geometry, or decided per item (-1).
+template <int ZC, int NT, bool FORCE, int BLK, int GT, int ST>
 __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, const WorkItem& it,
                                              unsigned char* smem) {
   constexpr int NW = BLK / 32;
@@ -438,9 +450,13 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
 #pragma unroll
     for (int k = 0; k < 7; ++k) red[k * BLK + threadIdx.x] = 0.0;
   }
-  const Geo geo = item_staged(it)
-                      ? stage_geometry<ZC>(S, atom0, Na, FORCE, smem + front)
-                      : Geo{S.g32 + bond0, S.ptype + bond0, S.rev_sm + bond0, S.NN + atom0, S.off + atom0, bond0, 0};
+  GeoT<ST> geo;
+  if (ST == 1 || (ST == -1 && item_staged(it))) {
+    const Geo s0 = stage_geometry<ZC>(S, atom0, Na, FORCE, smem + front);
+    geo = GeoT<ST>{s0.g, s0.pt, s0.rev, s0.nn, s0.boff, s0.bond0, s0.stride};
+  } else {
+    geo = GeoT<ST>{S.g32 + bond0, S.ptype + bond0, S.rev_sm + bond0, S.NN + atom0, S.off + atom0, bond0, 0};
+  }
   for (int base = warp * A; base < Na; base += NW * A) {
     const int il = base + aslot;
     // warp-uniform choice of the guard-free form (no divergence between the two)
@@ -500,24 +516,37 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
   fold_item(it, P, S.Nc, red, res);
 }
 
+// Energy/virial Tersoff items read their geometry through L1: staging it in shared memory
+// would cap the CTAs per SM without making the per-atom loads cheaper (measured).
+constexpr bool kStageEV = false;
+
 template <int ZC, int NT, bool FORCE, int BLK>
 __global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_batched(const JobView* __restrict__ jobs,
                                                        const WorkItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem[];
   const WorkItem it = items[blockIdx.x];
   if constexpr (!FORCE) {
-    tersoff_item<ZC, NT, FORCE, BLK, 32>(jobs, it, smem);  // energy/virial items: always 32 individuals
+    // energy/virial items: always 32 individuals (the run-time geometry form: the CSR-only
+    // specialisation spilled at this kernel's register bound and ran 5 % slower)
+    tersoff_item<ZC, NT, FORCE, BLK, 32, -1>(jobs, it, smem);
   } else if constexpr (ZC == 4) {
+    const bool st = item_staged(it);
+#define GPUGA_TI(GG)                                                     \
+  case GG:                                                               \
+    if (st) tersoff_item<ZC, NT, FORCE, BLK, GG, 1>(jobs, it, smem);     \
+    else tersoff_item<ZC, NT, FORCE, BLK, GG, 0>(jobs, it, smem);        \
+    break;
     switch (item_G(it)) {
-      case 32: tersoff_item<ZC, NT, FORCE, BLK, 32>(jobs, it, smem); break;
-      case 16: tersoff_item<ZC, NT, FORCE, BLK, 16>(jobs, it, smem); break;
-      case 8: tersoff_item<ZC, NT, FORCE, BLK, 8>(jobs, it, smem); break;
-      case 4: tersoff_item<ZC, NT, FORCE, BLK, 4>(jobs, it, smem); break;
-      case 2: tersoff_item<ZC, NT, FORCE, BLK, 2>(jobs, it, smem); break;
-      default: tersoff_item<ZC, NT, FORCE, BLK, 1>(jobs, it, smem); break;
+      GPUGA_TI(32)
+      GPUGA_TI(16)
+      GPUGA_TI(8)
+      GPUGA_TI(4)
+      GPUGA_TI(2)
+      default: GPUGA_TI(1)
     }
+#undef GPUGA_TI
   } else {
-    tersoff_item<ZC, NT, FORCE, BLK, 0>(jobs, it, smem);
+    tersoff_item<ZC, NT, FORCE, BLK, 0, -1>(jobs, it, smem);
   }
 }
 
@@ -952,10 +981,8 @@ constexpr size_t kRedBytes = (size_t)kWarps * 32 * kResK * sizeof(double);
 size_t force_smem_target(int zc) { return zc == 4 ? 72 * 1024 : 96 * 1024; }
 size_t stage_target(int zc) { return zc == 4 ? 74 * 1024 : 110 * 1024; }  // force scratch + staged geometry
 // Energy/virial Tersoff items run in 128-thread CTAs (more resident warps per SM at ~115
-// registers per thread) and read their geometry through L1: staging it in shared memory
-// would cap the CTAs per SM without making the per-atom loads cheaper (measured).
+// registers per thread); kStageEV (above) keeps their geometry in place.
 constexpr int kBlockEV = 128;
-constexpr bool kStageEV = false;
 constexpr size_t kSmemMax = 220 * 1024;
 
 int zclass_of(int z) { return z <= 4 ? 4 : (z <= 8 ? 8 : (z <= 16 ? 16 : 0)); }
