@@ -199,10 +199,12 @@ __host__ __device__ __forceinline__ int pack_G(int G, bool staged, size_t fbytes
 // of the same individual (l mod G) adds across atom slots.  Both partners of a
 // butterfly step form the same sum, so the result is deterministic, and every chain is
 // short (a sequential fold over 32/G atom slots per warp stalled the CTA).
+// GT: G as a compile-time constant (0: read from the item).
+template <int GT>
 __device__ __forceinline__ void fold_item(const WorkItem& it, int P, int Nc, const double* red,
                                           double* __restrict__ res) {
   __syncthreads();
-  const int G = item_G(it), nw = blockDim.x >> 5;
+  const int G = GT ? GT : item_G(it), nw = blockDim.x >> 5;
   const int lane = threadIdx.x & 31;
   for (int k = threadIdx.x >> 5; k < kResK; k += nw) {
     double s = 0.0;
@@ -214,13 +216,14 @@ __device__ __forceinline__ void fold_item(const WorkItem& it, int P, int Nc, con
 }
 
 // Same for partial sums held in registers (they are first written out).
+template <int GT>
 __device__ __forceinline__ void reduce_item(const WorkItem& it, int P, int Nc, double (&acc)[kResK],
                                             unsigned char* smem, double* __restrict__ res) {
   __syncthreads();
   double* red = reinterpret_cast<double*>(smem);
 #pragma unroll
   for (int k = 0; k < kResK; ++k) red[(size_t)k * blockDim.x + threadIdx.x] = acc[k];
-  fold_item(it, P, Nc, red, res);
+  fold_item<GT>(it, P, Nc, red, res);
 }
 
 // Geometry of one configuration as a CTA sees it.  Unstaged: the global CSR
@@ -474,7 +477,7 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
   }
   if (!FORCE) {
     red[7 * BLK + threadIdx.x] = 0.0;
-    fold_item(it, P, S.Nc, red, res);
+    fold_item<GT>(it, P, S.Nc, red, res);
     return;
   }
   __syncthreads();
@@ -513,7 +516,7 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
 #pragma unroll
   for (int k = 0; k < 7; ++k) red[k * BLK + threadIdx.x] = 0.0;
   red[7 * BLK + threadIdx.x] = ferr;
-  fold_item(it, P, S.Nc, red, res);
+  fold_item<GT>(it, P, S.Nc, red, res);
 }
 
 // Energy/virial Tersoff items read their geometry through L1: staging it in shared memory
@@ -744,15 +747,6 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
   const Consts kc{J.consts, Pstride, pl};
   RIC R;
   if (KIND == 1) load_ri(kc, R);
-  const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
-  const int N = S.N;
-  double acc[kResK];
-#pragma unroll
-  for (int k = 0; k < kResK; ++k) acc[k] = 0.0;
-  // RI self energy: an energy item covers all atoms of its configuration, so warp 0 adds
-  // -K_C q^2 S sum_i (q_i / q)^2 once per individual, in FP64
-  if (KIND == 1 && !FORCE && J.ri_self && warp == 0)
-    acc[0] = -((double)kc[RC_SELF] + (double)kc[RC_SELFLO]) * S.ri_qsum[c];
   float* wsm = reinterpret_cast<float*>(smem + (size_t)kWarps * 32 * kResK * sizeof(double));
   if (KIND == 2) {
     for (size_t t = threadIdx.x; t < NNSmem<NMAX>::floats; t += blockDim.x) wsm[t] = 0.f;  // zero padding
@@ -764,6 +758,15 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
     }
     __syncthreads();
   }
+  const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
+  const int N = S.N;
+  double acc[kResK];
+#pragma unroll
+  for (int k = 0; k < kResK; ++k) acc[k] = 0.0;
+  // RI self energy: an energy item covers all atoms of its configuration, so warp 0 adds
+  // -K_C q^2 S sum_i (q_i / q)^2 once per individual, in FP64
+  if (KIND == 1 && !FORCE && J.ri_self && warp == 0)
+    acc[0] = -((double)kc[RC_SELF] + (double)kc[RC_SELFLO]) * S.ri_qsum[c];
   // per-atom sums over the atom's pairs: compensated FP32 (Kahan), added to the
   // FP64 accumulators once per atom -- a per-pair FP64 add would cost two
   // FP32->FP64 conversions per term, which run at a fraction of the FP32 rate
@@ -920,7 +923,7 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
       finish_atom(il, ks);
     }
   }
-  reduce_item(it, P, S.Nc, acc, smem, res);
+  reduce_item<32>(it, P, S.Nc, acc, smem, res);  // pair items hold 32 individuals
 }
 
 // --------------------------------------------------------------------------- fitness
