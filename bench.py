@@ -514,7 +514,10 @@ def run_serving(args) -> dict:
             "peak_resident_jobs": st["peak_resident_jobs"], "generation_batches": st["batches"],
             "total_units": total_units, "arrivals": "Poisson, 2 jobs/s",
             "one_at_a_time_plain_fp64_s_estimate": serial_plain_s,
+            # wall time includes the Poisson arrival gaps (about 16 s for 32 jobs at 2 jobs/s)
             "speedup_vs_one_at_a_time_plain_fp64": serial_plain_s / max(wall, 1e-9),
+            "busy_s": total_units / max(st["evals_per_s"], 1e-9),
+            "speedup_busy_vs_one_at_a_time_plain_fp64": serial_plain_s * st["evals_per_s"] / max(total_units, 1),
             "data": "synthetic (workloads 1-3, 20-500 configurations, teacher targets)"}
 
 
