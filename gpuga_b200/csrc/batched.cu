@@ -39,9 +39,15 @@ namespace gpuga {
 
 // ----------------------------------------------------------------- per-individual constants
 // Tersoff (minimal_tersoff.cu:39-75): per pair set s: lr = sqrt(2S)*A, la = sqrt(2/S)*A,
-// cr = D0/(S-1), ca = S*D0/(S-1), r0; then n, beta, h, R1, R2, pi/(R2-R1), -1/(2n).
+// cr = D0/(S-1), ca = S*D0/(S-1), r0; then n, beta, h, R1, R2, pi/(R2-R1), -1/(2n); then the
+// FP64 remainders of lr, la, cr, ca and -1/(2n).  The FP32 rounding of these derived constants
+// is the same for every bond of an individual, so it does not average out: cr, ca and lr, la
+// enter fr' - b fa', which cancels near equilibrium, and -1/(2n) every bond order.  Without
+// the remainders the fitness of a parameter set with S != 2 was off by up to 1e-5 relative.
 enum { TC_LR = 0, TC_LA = 2, TC_CR = 4, TC_CA = 6, TC_R0 = 8, TC_EN = 10, TC_BETA, TC_H, TC_R1, TC_R2, TC_PF,
-       TC_MHON, TC_COUNT };
+       TC_MHON, TC_LRL, TC_LAL = TC_LRL + 2, TC_CRL = TC_LAL + 2, TC_CAL = TC_CRL + 2, TC_MHONL = TC_CAL + 2,
+       TC_COUNT };
+static_assert(TC_COUNT <= kMaxConsts, "per-individual Tersoff constants");
 // RI (ri.cu:36-110): qq[3], a[3], b[3] = 1/rho, c[3], rc, v_rc, dv_rc, Morse lr, la, cr, ca, r0,
 // then the FP64 remainders of b[3], lr and la (their FP32 roundings would otherwise shift the
 // exponents |d/rho|, |lr (d - r0)| of up to ~20 by 2^-24 relative), and the self-energy
@@ -87,6 +93,10 @@ __global__ void decode_jobs(const JobView* __restrict__ jobs, const int2* __rest
       put(TC_CR + s, D0 / (S - 1.0));
       put(TC_CA + s, S * D0 / (S - 1.0));
       put(TC_R0 + s, R0);
+      put_lo(TC_LRL + s, sqrt(2.0 * S) * A);
+      put_lo(TC_LAL + s, sqrt(2.0 / S) * A);
+      put_lo(TC_CRL + s, D0 / (S - 1.0));
+      put_lo(TC_CAL + s, S * D0 / (S - 1.0));
     }
     const double en = par(4 + off), R1 = par(7 + off), R2 = par(8 + off);
     put(TC_EN, en);
@@ -96,6 +106,7 @@ __global__ void decode_jobs(const JobView* __restrict__ jobs, const int2* __rest
     put(TC_R2, R2);
     put(TC_PF, M_PI / (R2 - R1));
     put(TC_MHON, -0.5 / en);
+    put_lo(TC_MHONL, -0.5 / en);
   } else if (is_ri_type(potential_type)) {
     const double q0 = par(0), ratio = ri_charge_ratio(potential_type);
     const double kc = 14.399645;  // ri.cu:29
@@ -144,9 +155,12 @@ struct Consts {
 // --------------------------------------------------------------------------- Tersoff
 struct TersoffC {
   float lr[2], la[2], cr[2], ca[2], r0[2];
-  float en, beta, h, r1, r2, pf, mhon;
+  float lrl[2], lal[2], crl[2], cal[2];  // FP64 remainders of lr, la, cr, ca
+  float en, beta, h, r1, r2, pf, mhon, mhonl;
 };
 
+// LO: also load the FP64 remainders of lr, la, cr, ca (the remainder of -1/(2n) always).
+template <bool LO>
 __device__ __forceinline__ void load_tersoff(const Consts& k, TersoffC& C) {
 #pragma unroll
   for (int s = 0; s < 2; ++s) {
@@ -155,6 +169,12 @@ __device__ __forceinline__ void load_tersoff(const Consts& k, TersoffC& C) {
     C.cr[s] = k[TC_CR + s];
     C.ca[s] = k[TC_CA + s];
     C.r0[s] = k[TC_R0 + s];
+    if (LO) {
+      C.lrl[s] = k[TC_LRL + s];
+      C.lal[s] = k[TC_LAL + s];
+      C.crl[s] = k[TC_CRL + s];
+      C.cal[s] = k[TC_CAL + s];
+    }
   }
   C.en = k[TC_EN];
   C.beta = k[TC_BETA];
@@ -163,6 +183,7 @@ __device__ __forceinline__ void load_tersoff(const Consts& k, TersoffC& C) {
   C.r2 = k[TC_R2];
   C.pf = k[TC_PF];
   C.mhon = k[TC_MHON];
+  C.mhonl = k[TC_MHONL];
 }
 
 // cutoff function of minimal_tersoff.cu:77-90
@@ -289,7 +310,7 @@ __device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int N
 //
 // FULL: every one of the ZC bond slots is present (Z == ZC, e.g. all atoms of a diamond
 // lattice), so that the per-slot guards fold away at compile time.
-template <int ZC, int NT, bool FORCE, bool FULL, class GEO>
+template <int ZC, int NT, bool FORCE, bool FULL, bool LO, class GEO>
 __device__ __forceinline__ float tersoff_atom(const GEO& geo, const TersoffC& C, int il, int Na, float* fsm, int G,
                                               int g, float (&v)[6]) {
   const int Z = FULL ? ZC : geo.nn[il];
@@ -319,8 +340,16 @@ __device__ __forceinline__ float tersoff_atom(const GEO& geo, const TersoffC& C,
     if (j < Z) {
       const int s = NT == 2 ? st[j] : 0;
       const float t = dd[j] - (s ? C.r0[1] : C.r0[0]);
-      fr[j] = (s ? C.cr[1] : C.cr[0]) * expf(-(s ? C.lr[1] : C.lr[0]) * t);
-      fa[j] = (s ? C.ca[1] : C.ca[0]) * expf(-(s ? C.la[1] : C.la[0]) * t);
+      const float cr = s ? C.cr[1] : C.cr[0], ca = s ? C.ca[1] : C.ca[0];
+      const float er = expf(-(s ? C.lr[1] : C.lr[0]) * t), ea = expf(-(s ? C.la[1] : C.la[0]) * t);
+      if constexpr (LO) {
+        // c e^{-l t} with c = c_h + c_l, l = l_h + l_l:  c_h E + (c_l - c_h l_l t) E, E = e^{-l_h t}
+        fr[j] = fmaf(fmaf(-cr * (s ? C.lrl[1] : C.lrl[0]), t, s ? C.crl[1] : C.crl[0]), er, cr * er);
+        fa[j] = fmaf(fmaf(-ca * (s ? C.lal[1] : C.lal[0]), t, s ? C.cal[1] : C.cal[0]), ea, ca * ea);
+      } else {
+        fr[j] = cr * er;
+        fa[j] = ca * ea;
+      }
       cutoff_fn(C.r1, C.r2, C.pf, dd[j], fc[j], fcp[j]);
     }
   }
@@ -359,14 +388,17 @@ __device__ __forceinline__ float tersoff_atom(const GEO& geo, const TersoffC& C,
       if (!(zeta < 1.0e-16f)) {  // minimal_tersoff.cu:178-185
         const float zn = powf_dd(zeta, C.en);
         const float opz = 1.0f + zn;
-        b = powf_dd(opz, C.mhon);
+        b = powf_dd(opz, C.mhon, C.mhonl);
         bp = __fdividef(-0.5f * b * zn, opz * zeta);
       }
       const int s = NT == 2 ? st[j] : 0;
       const float e = fr[j] - b * fa[j];
       pe = fmaf(0.5f * fc[j], e, pe);
-      const float frp = -(s ? C.lr[1] : C.lr[0]) * fr[j];
-      const float fap = -(s ? C.la[1] : C.la[0]) * fa[j];
+      float frp = -(s ? C.lr[1] : C.lr[0]) * fr[j], fap = -(s ? C.la[1] : C.la[0]) * fa[j];
+      if constexpr (LO) {
+        frp = fmaf(-(s ? C.lrl[1] : C.lrl[0]), fr[j], frp);
+        fap = fmaf(-(s ? C.lal[1] : C.lal[0]), fa[j], fap);
+      }
       Ap[j] = fcp[j] * e + fc[j] * (frp - b * fap);
       Sb[j] = bp * fa[j];
       Tb[j] = Sb[j] * fc[j];
@@ -426,7 +458,7 @@ __device__ __forceinline__ float tersoff_atom(const GEO& geo, const TersoffC& C,
 // GT: the item's individuals per item G as a compile-time constant (0: read from the item), so
 // that the force scratch addressing and the atom-slot split fold into shifts and constants;
 // ST: staged (1) or in-place CSR (0) geometry, or decided per item (-1).
-template <int ZC, int NT, bool FORCE, int BLK, int GT, int ST>
+template <int ZC, int NT, bool FORCE, int BLK, int GT, int ST, bool LO>
 __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, const WorkItem& it,
                                              unsigned char* smem) {
   constexpr int NW = BLK / 32;
@@ -441,7 +473,7 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
   const int p = it.p0 + g;
   const Consts kc{J.consts, J.Pstride, p < P ? p : it.p0};
   TersoffC C;
-  load_tersoff(kc, C);
+  load_tersoff<LO>(kc, C);
   const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
   const int bond0 = S.off[atom0];
   // force scratch: shared memory, or for configurations too large for it the item's own
@@ -466,8 +498,8 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
     const bool full = __all_sync(0xffffffffu, il >= Na || geo.nn[il] == ZC);
     if (il < Na) {
       float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      const float pe = full ? tersoff_atom<ZC, NT, FORCE, true>(geo, C, il, Na, fsm, G, g, v)
-                            : tersoff_atom<ZC, NT, FORCE, false>(geo, C, il, Na, fsm, G, g, v);
+      const float pe = full ? tersoff_atom<ZC, NT, FORCE, true, LO>(geo, C, il, Na, fsm, G, g, v)
+                            : tersoff_atom<ZC, NT, FORCE, false, LO>(geo, C, il, Na, fsm, G, g, v);
       if (!FORCE) {
         red[threadIdx.x] += (double)pe;
 #pragma unroll
@@ -523,7 +555,8 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
 // would cap the CTAs per SM without making the per-atom loads cheaper (measured).
 constexpr bool kStageEV = false;
 
-template <int ZC, int NT, bool FORCE, int BLK>
+// LO: the job's derived constants need their FP64 remainders (tersoff_consts_exact).
+template <int ZC, int NT, bool FORCE, int BLK, bool LO>
 __global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_batched(const JobView* __restrict__ jobs,
                                                        const WorkItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -531,13 +564,13 @@ __global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_ba
   if constexpr (!FORCE) {
     // energy/virial items: always 32 individuals (the run-time geometry form: the CSR-only
     // specialisation spilled at this kernel's register bound and ran 5 % slower)
-    tersoff_item<ZC, NT, FORCE, BLK, 32, -1>(jobs, it, smem);
+    tersoff_item<ZC, NT, FORCE, BLK, 32, -1, LO>(jobs, it, smem);
   } else if constexpr (ZC == 4) {
     const bool st = item_staged(it);
 #define GPUGA_TI(GG)                                                     \
   case GG:                                                               \
-    if (st) tersoff_item<ZC, NT, FORCE, BLK, GG, 1>(jobs, it, smem);     \
-    else tersoff_item<ZC, NT, FORCE, BLK, GG, 0>(jobs, it, smem);        \
+    if (st) tersoff_item<ZC, NT, FORCE, BLK, GG, 1, LO>(jobs, it, smem);     \
+    else tersoff_item<ZC, NT, FORCE, BLK, GG, 0, LO>(jobs, it, smem);        \
     break;
     switch (item_G(it)) {
       GPUGA_TI(32)
@@ -549,7 +582,7 @@ __global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_ba
     }
 #undef GPUGA_TI
   } else {
-    tersoff_item<ZC, NT, FORCE, BLK, 0, -1>(jobs, it, smem);
+    tersoff_item<ZC, NT, FORCE, BLK, 0, -1, LO>(jobs, it, smem);
   }
 }
 
@@ -1074,11 +1107,30 @@ struct ItemSpec {
   double cost, units, flops, sfu;
 };
 struct LaunchKey {
-  int kind, zclass, nmax, force;
+  int kind, zclass, nmax, force, lo;
   bool operator<(const LaunchKey& o) const {
-    return std::tie(kind, zclass, nmax, force) < std::tie(o.kind, o.zclass, o.nmax, o.force);
+    return std::tie(kind, zclass, nmax, force, lo) < std::tie(o.kind, o.zclass, o.nmax, o.force, o.lo);
   }
 };
+
+// True when every derived Tersoff constant of every individual is exact in FP32: S fixed by its
+// bounds and sqrt(2S), sqrt(2/S), 1/(S-1), S/(S-1) powers of two (S = 2, the common choice), so
+// that lr, la, cr, ca are FP32 parameters times powers of two.  Otherwise the kernels carry the
+// constants' FP64 remainders (the LO instantiation).
+bool tersoff_consts_exact(const PotentialSpec& sp, int num_types) {
+  auto pow2 = [](double v) {
+    int e;
+    return v > 0 && std::isfinite(v) && std::frexp(v, &e) == 0.5;
+  };
+  for (int s = 0; s < num_types; ++s) {
+    const int m = 4 * s + 3;
+    if ((int)sp.pmin.size() <= m || sp.pmin[m] != sp.pmax[m]) return false;
+    const double S = sp.pmin[m];
+    if (!(pow2(std::sqrt(2.0 * S)) && pow2(std::sqrt(2.0 / S)) && pow2(1.0 / (S - 1.0)) && pow2(S / (S - 1.0))))
+      return false;
+  }
+  return true;
+}
 
 // Work items of one job, grouped by kernel.
 //   Algorithmic work per (individual, atom), counted on the batched formulation
@@ -1095,6 +1147,7 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
   const int kind = tersoff ? 0 : (is_ri_type(d.potential_type) ? 1 : 2);
   // NN2B: register-array size of the MLP; Tersoff: number of atom types (kernel template)
   const int nmax = kind == 2 ? nmax_of(d.num_neurons) : (kind == 0 ? d.num_types : 0);
+  const bool lo = kind == 0 && !tersoff_consts_exact(e->spec, d.num_types);
   if (kind == 2 && nmax == 0) {
     set_error("batched NN2B supports up to 32 neurons per layer (got %d).", d.num_neurons);
     return GPUGA_ERR_UNSUPPORTED;
@@ -1165,7 +1218,7 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
     } else {
       smem += kPairStageBytes;  // RI: the warps' two-stage pair buffers
     }
-    const LaunchKey key{kind, zc, nmax, force ? 1 : 0};
+    const LaunchKey key{kind, zc, nmax, force ? 1 : 0, lo ? 1 : 0};
     smem_need[key] = std::max(smem_need[key], smem);
     double cf = 0, cs = 0;
     const bool half = kind != 0 && !force;
@@ -1207,10 +1260,14 @@ int launch_one(const LaunchSet* ls, const Launch& L, cudaStream_t st, bool confi
   do {                                                                                  \
     constexpr int BLK = F ? kBlock : kBlockEV;                                          \
     if (configure_only) {                                                               \
-      GPUGA_TRY(set_smem(tersoff_batched<ZC, NT, F, BLK>));                             \
+      if (L.lo) GPUGA_TRY(set_smem(tersoff_batched<ZC, NT, F, BLK, true>));             \
+      else GPUGA_TRY(set_smem(tersoff_batched<ZC, NT, F, BLK, false>));                 \
       break;                                                                            \
     }                                                                                   \
-    tersoff_batched<ZC, NT, F, BLK><<<grid, dim3(BLK), L.smem, st>>>(ls->d_jobs, items); \
+    if (L.lo)                                                                           \
+      tersoff_batched<ZC, NT, F, BLK, true><<<grid, dim3(BLK), L.smem, st>>>(ls->d_jobs, items); \
+    else                                                                                \
+      tersoff_batched<ZC, NT, F, BLK, false><<<grid, dim3(BLK), L.smem, st>>>(ls->d_jobs, items); \
   } while (0)
 #define GPUGA_TERSOFF(ZC, F)                                                          \
   do {                                                                                \
@@ -1276,6 +1333,7 @@ int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSe
     L.kind = kv.first.kind;
     L.zclass = kv.first.zclass;
     L.nmax = kv.first.nmax;
+    L.lo = kv.first.lo != 0;
     L.force = kv.first.force != 0;
     L.smem = smem_need[kv.first];
     L.count = (int)v.size();

@@ -130,6 +130,7 @@ struct Launch {
   int zclass = 4;      // Tersoff register-array size
   int nmax = 0;        // NN2B register-array size; Tersoff: number of atom types
   bool force = false;  // force items (gather pass) vs energy/virial items
+  bool lo = false;     // Tersoff: carry the FP64 remainders of the derived constants
   size_t smem = 0;
   int count = 0;
   size_t first = 0;    // offset of the launch's items in the set's item array

@@ -61,7 +61,7 @@ GPUGA_HD float pdd_rcp(float t) {
 #endif
 }
 
-GPUGA_HD float powf_dd(float x, float y) {
+GPUGA_HD float powf_dd(float x, float y, float y_lo = 0.0f) {
   if (x != x) return x;  // NaN
   // x = 2^e m with m in [sqrt(1/2), sqrt(2))
   const int32_t ix = pdd_as_int(x);
@@ -97,6 +97,7 @@ GPUGA_HD float powf_dd(float x, float y) {
   const float t_h = y * L_h;
   float t_l = fmaf(y, L_h, -t_h);
   t_l = fmaf(y, L_l, t_l);
+  t_l = fmaf(y_lo, L_h, t_l);  // y = y + y_lo when the exponent itself is a rounded FP64 value
   // 2^t = 2^k 2^r (out of range: selected away at the end, no branch)
   const float k = rintf(t_h);
   const float r = (t_h - k) + t_l;
