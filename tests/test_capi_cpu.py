@@ -139,3 +139,15 @@ def test_synthetic_sets_parse(tmp_path):
         st, sz = parse(d)
         assert st == 0, _lib.load().gpuga_last_error()
         assert sz[3] == Nc and sz[4] == Nc // 2 and sz[5] == int(data["Na"].sum())
+
+
+def test_cli_rejects_unknown_options_with_usage():
+    """The gpuga driver parses its options before touching a GPU: an unknown one prints the usage."""
+    import os
+    import subprocess
+    if not os.path.exists(_lib.CLI_PATH):
+        pytest.skip("gpuga CLI not built")
+    r = subprocess.run([_lib.CLI_PATH, "--no-such-option"], input="0\n", capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2
+    for opt in ("--host-loop", "--ri-self-energy", "--nn2b-taper", "--neighbor-cells"):
+        assert opt in r.stderr

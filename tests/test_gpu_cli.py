@@ -39,3 +39,21 @@ def test_cli_reports_input_errors(tmp_path):
     r = subprocess.run([_lib.CLI_PATH], input=f"1\n{tmp_path}\n", capture_output=True, text=True, timeout=120)
     assert r.returncode == 1
     assert "potential.in" in r.stderr
+
+
+def test_cli_host_loop_matches_device_loop(built_oracle, tmp_path):
+    """--host-loop (selection on the host each generation) writes the same ga.out as the default
+    device-resident GA loop."""
+    import shutil
+    d, _ = synthetic_dir(built_oracle, 1, 6, str(tmp_path / "a"))
+    with open(os.path.join(d, "ga.in"), "w") as f:
+        f.write("maximum_generation 12\npopulation_size 40\nparent_number 20\nmutation_rate 0.2\n")
+    d2 = str(tmp_path / "b")
+    shutil.copytree(d, d2)
+    outs = []
+    for dd, extra in ((d, []), (d2, ["--host-loop"])):
+        r = subprocess.run([_lib.CLI_PATH, "--seed", "7"] + extra, input=f"1\n{dd}\n", capture_output=True,
+                           text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        outs.append(open(os.path.join(dd, "ga.out")).read())
+    assert outs[0] == outs[1]
