@@ -45,3 +45,33 @@ def test_random_population_error_tail(S_free, tol):
     if not np.array_equal(order, oorder):
         srt = np.sort(f64)
         assert (np.diff(srt) / np.abs(srt[1:])).min() <= 2 * tol
+
+
+@pytest.mark.parametrize("cutoff,zmax", [(3.0, 4), (3.9, 16)])
+def test_free_S_and_wide_lists_against_the_oracle(built_oracle, tmp_path, cutoff, zmax):
+    """The instantiation that carries the constants' remainders (S free), on 4-neighbor lists and on
+    up to 16-neighbor lists (cutoff 3.9 A: the second shell enters the list with fc = 0 beyond R2), against
+    the FP64 oracle: relative fitness error <= 2e-5, per-config virials <= 2e-6 of scale."""
+    from tests.helpers import oracle_targets
+    data = synth.make(2, Nc=24, seed=31)
+    data["cutoff"] = cutoff
+    data["pmin"][3], data["pmax"][3] = 1.5, 2.5
+    data["teacher01"][3] = 0.37
+    data = synth.fill_targets(data, oracle_targets(built_oracle))
+    d = synth.write_dir(data, str(tmp_path / "set"))
+    s = built_oracle.OracleSet(d)
+    P = 40
+    pop = synth.population(data, P, seed=8)
+    with Fitness(d) as e:
+        NN, _ = e.neighbors()
+        assert zmax // 2 < int(NN.max()) <= zmax  # the 4- or 16-slot kernel class
+        fit = np.asarray(e.compute(P, pop))
+        E, W, _ = e.config_results(P)
+    ofit = s.fitness(pop)
+    assert (np.abs(fit - ofit) / np.abs(ofit)).max() <= 2e-5
+    Ncf = s.Nc_force
+    for p in (0, P - 1):
+        oF, oW, ope = s.find_force(s.decode(pop[p]))
+        _, oWc = s.config_sums(oW, ope)
+        oWm = oWc.reshape(6, s.Nc).T
+        assert np.abs(W[p, Ncf:] - oWm[Ncf:]).max() <= 2e-6 * np.abs(oWm[Ncf:]).max()
