@@ -1117,21 +1117,15 @@ struct LaunchKey {
   }
 };
 
-// True when every derived Tersoff constant of every individual is exact in FP32: S fixed by its
-// bounds and sqrt(2S), sqrt(2/S), 1/(S-1), S/(S-1) powers of two (S = 2, the common choice), so
-// that lr, la, cr, ca are FP32 parameters times powers of two.  Otherwise the kernels carry the
-// constants' FP64 remainders (the LO instantiation).
+// True when every derived Tersoff constant of every individual is exact in FP32: S fixed at 2 by
+// its bounds, so that lr = 2A, la = A, cr = D0, ca = 2 D0 are FP32 parameters times powers of two.
+// (S = 2 is the only such value: sqrt(2S) sqrt(2/S) = 2 leaves S = 2^(2a-1) for powers of two, and
+// S - 1 a power of two only for a = 1.)  Otherwise the kernels carry the constants' FP64
+// remainders (the LO instantiation).
 bool tersoff_consts_exact(const PotentialSpec& sp, int num_types) {
-  auto pow2 = [](double v) {
-    int e;
-    return v > 0 && std::isfinite(v) && std::frexp(v, &e) == 0.5;
-  };
   for (int s = 0; s < num_types; ++s) {
     const int m = 4 * s + 3;
-    if ((int)sp.pmin.size() <= m || sp.pmin[m] != sp.pmax[m]) return false;
-    const double S = sp.pmin[m];
-    if (!(pow2(std::sqrt(2.0 * S)) && pow2(std::sqrt(2.0 / S)) && pow2(1.0 / (S - 1.0)) && pow2(S / (S - 1.0))))
-      return false;
+    if ((int)sp.pmin.size() <= m || sp.pmin[m] != 2.0f || sp.pmax[m] != 2.0f) return false;
   }
   return true;
 }
