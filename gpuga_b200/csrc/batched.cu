@@ -906,7 +906,7 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
       const int k1 = min(max(q_s1[st] - b0, 0), n), k2 = min(max(q_s2[st] - b0, 0), n);
       auto run = [&](auto type, int kb, int ke) {
         constexpr int T = decltype(type)::value;
-#pragma unroll 2
+#pragma unroll 4  // four pairs' shared-memory loads in flight (2 measured 1 % slower)
         for (int k = kb; k < ke; ++k) {
           const float4 q = g[k];
           float p2, fd;
