@@ -1122,7 +1122,7 @@ struct LaunchKey {
 // (S = 2 is the only such value: sqrt(2S) sqrt(2/S) = 2 leaves S = 2^(2a-1) for powers of two, and
 // S - 1 a power of two only for a = 1.)  Otherwise the kernels carry the constants' FP64
 // remainders (the LO instantiation).
-bool tersoff_consts_exact(const PotentialSpec& sp, int num_types) {
+static bool tersoff_consts_exact(const PotentialSpec& sp, int num_types) {
   for (int s = 0; s < num_types; ++s) {
     const int m = 4 * s + 3;
     if ((int)sp.pmin.size() <= m || sp.pmin[m] != 2.0f || sp.pmax[m] != 2.0f) return false;
