@@ -60,6 +60,9 @@ def parse_args():
     ap.add_argument("--serving", action="store_true", help="serving benchmark (workload 5) instead")
     ap.add_argument("--serving-jobs", type=int, default=32)
     ap.add_argument("--serving-generations", type=int, default=20)
+    ap.add_argument("--serving-seconds", type=float, default=4.0,
+                    help="bounded serving block: seconds every job keeps running after the last arrival")
+    ap.add_argument("--no-serving", action="store_true", help="skip the bounded serving block")
     ap.add_argument("--ga-generations", type=int, default=20,
                     help="generations of the full GA loop timed on the host and on the device loop (0 = skip)")
     return ap.parse_args()
@@ -356,12 +359,8 @@ def run_ours(args, dist: Dist):
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": nsteps, "warmup": nwarm,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 pair/3-body math, f64 accumulation", "data": "synthetic (seeded generator, teacher targets)",
-        "config": {"workload": f"batched minimal-Tersoff Si: {e.Nc} diamond configs of 8/64/216/512 atoms"
-                               if args.workload == 2 else data["name"],
-                   "population": P, "configs": e.Nc, "atoms": Natoms, "bonds": e.num_bonds,
-                   "units_per_step": P * Natoms, "l2": "flushed between steps (256 MiB write, outside the step events)",
-                   "parallelism": f"replicas{dist.world} (population per GPU, weak)"},
+        "dtype": "f32 pair/3-body math, f64 accumulation", "data": DATA,
+        "config": workload_config(args, data, P, e.Nc, Natoms, e.num_bonds, dist.world),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": P * d * 4,
                 "d2h_bytes_per_step": P * 8 * 4, "latency_ms": {"p50": p50, "p99": p99}},
         "gpu_launches": kernels_per_step * nsteps,
@@ -378,6 +377,9 @@ def run_ours(args, dist: Dist):
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(data, args.cpu_seconds)
     e.close()
+    if dist.world == 1 and not args.no_serving:
+        # bounded serving block (32 jobs of workloads 1-3, Poisson arrivals), a single-GPU feature
+        result["serving"] = run_serving(args, steady=True)
     return result
 
 
@@ -430,6 +432,18 @@ def cpu_baseline(data, budget_s: float) -> dict:
 
 
 # ----------------------------------------------------------------------------- reference arm
+DATA = "synthetic (seeded generator, teacher targets)"
+
+
+def workload_config(args, data, P, Nc, N, bonds, world) -> dict:
+    """The `config` object of both arms (same keys and values for the same workload)."""
+    name = (f"batched minimal-Tersoff Si: {Nc} diamond configs of 8/64/216/512 atoms" if args.workload == 2
+            else data["name"])
+    return {"workload": name, "population": P, "configs": Nc, "atoms": N, "bonds": bonds,
+            "units_per_step": P * N, "l2": "flushed between steps (256 MiB write, outside the step timing)",
+            "parallelism": f"replicas{world} (population per GPU, weak)"}
+
+
 def run_reference(args, dist: Dist):
     probe = os.path.join(ROOT, "oracle", "_ref", "ref_probe")
     if dist.rank != 0:
@@ -447,6 +461,8 @@ def run_reference(args, dist: Dist):
     d = synth.write_dir(data, tempfile.mkdtemp(prefix="gpuga_ref_"))
     P = int(data["ga"]["population_size"])
     N = int(data["Na"].sum())
+    from oracle import oracle
+    bonds = oracle.OracleSet(d).num_bonds  # the same neighbor rule as the engine (bit-exact lists)
     r = subprocess.run([probe, "time", d, str(P), str(args.steps), str(max(args.warmup, 3)), "12345678"],
                        capture_output=True, text=True, timeout=3000)
     shutil.rmtree(d, ignore_errors=True)
@@ -461,26 +477,19 @@ def run_reference(args, dist: Dist):
               f"Fitness::compute, P={P}, {N} atoms, {len(ms)} generations on the GPU, wall time per generation")
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": len(ms),
             "warmup": max(args.warmup, 3), "ms_per_step": sum(ms) / len(ms), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (fast-math)", "data": "synthetic",
-            "config": {"workload": "batched minimal-Tersoff Si" if args.workload == 2 else data["name"],
-                       "population": P, "atoms": N, "l2": "flushed between steps (256 MiB memset)"},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (fast-math)", "data": DATA,
+            "config": workload_config(args, data, P, len(data["Na"]), N, bonds, 1),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))}}
 
 
 # ----------------------------------------------------------------------------- serving
-def run_serving(args) -> dict:
-    """Continuous batching: 32 fitting jobs drawn from workloads 1-3 (20..500 configurations each)
-    arriving as a Poisson process (2 jobs/s) into a server with a 120 GB budget.  Reports the
-    aggregate evals/s, p50/p99 generation latency and the one-job-at-a-time plain-FP64 estimate."""
-    import random
-
-    from gpuga_b200 import PATH_PLAIN64, Fitness, Server, synth
-    rng = random.Random(5)
-    gens = args.serving_generations
-    jobs = []
-    plain_rate = {}
+def _serving_jobs(args, rng):
+    """Job directories of the serving mix: workloads 1-3 with 20..500 configurations, seeded synthetic
+    data with teacher targets; plus the plain FP64 one-individual-per-launch rate of each potential."""
+    from gpuga_b200 import PATH_PLAIN64, Fitness, synth
+    jobs, plain_rate = [], {}
     tmp = tempfile.mkdtemp(prefix="gpuga_serving_")
     for k in range(args.serving_jobs):
         cfg = rng.choice([1, 2, 3])
@@ -488,7 +497,6 @@ def run_serving(args) -> dict:
         data = synth.make(cfg, seed=100 + k, Nc=Nc)
         with Fitness(arrays=data, **engine_opts(data, 0)) as e0:
             data = synth.fill_targets(data, lambda _d, p, e0=e0: e0.find_force64(p))
-            key = (cfg, Nc)
             if cfg not in plain_rate:  # plain FP64 one-individual-per-launch rate of this potential
                 pop = synth.population(data, 4, seed=1)
                 e0.compute(1, pop[:1], path=PATH_PLAIN64)
@@ -496,30 +504,59 @@ def run_serving(args) -> dict:
                 e0.compute(4, pop, path=PATH_PLAIN64)
                 plain_rate[cfg] = 4 * e0.N / (time.perf_counter() - t0)
         d = synth.write_dir(data, os.path.join(tmp, f"job{k}"))
-        P = int(data["ga"]["population_size"])
-        jobs.append((d, cfg, P, int(data["Na"].sum())))
+        jobs.append((d, cfg, int(data["ga"]["population_size"]), int(data["Na"].sum())))
+    return jobs, plain_rate, tmp
+
+
+def run_serving(args, steady: bool = False) -> dict:
+    """Continuous batching: 32 fitting jobs drawn from workloads 1-3 (20..500 configurations each)
+    arriving as a Poisson process (2 jobs/s) into a server with a 120 GB budget.  Reports the
+    aggregate evals/s, the per-generation latency (device time of a generation of all resident
+    jobs, and the wall-clock time per generation each job saw, stalls included) and the
+    one-job-at-a-time plain-FP64 estimate for the same work.
+
+    steady=False: every job runs --serving-generations generations.  steady=True (the bounded block
+    of the default benchmark): every job runs until --serving-seconds after the last arrival and is
+    then cancelled, so that all jobs are resident together for a while."""
+    import random
+
+    from gpuga_b200 import Server
+    rng = random.Random(5)
+    jobs, plain_rate, tmp = _serving_jobs(args, rng)
+    gens = 10 ** 6 if steady else args.serving_generations
     with Server(device=0, hbm_budget_bytes=120e9, max_jobs=32) as srv:
         t0 = time.perf_counter()
         ids = []
         for k, (d, cfg, P, N) in enumerate(jobs):
             ids.append(srv.submit(d, seed=1000 + k, generations=gens))
-            time.sleep(rng.expovariate(2.0))
+            if k + 1 < len(jobs):
+                time.sleep(rng.expovariate(2.0))
+        if steady:
+            time.sleep(args.serving_seconds)
+            for j in ids:
+                srv.cancel(j)
         rc = srv.drain(3000)
         wall = time.perf_counter() - t0
         st = srv.stats()
+        done = [srv.poll(j)[1] for j in ids]
     shutil.rmtree(tmp, ignore_errors=True)
-    total_units = sum(P * N * gens for _, _, P, N in jobs)
-    serial_plain_s = sum(P * N * gens / plain_rate[cfg] for _, cfg, P, N in jobs)
+    units = [P * N * g for (_, _, P, N), g in zip(jobs, done)]
+    total_units = float(sum(units))
+    serial_plain_s = sum(u / plain_rate[cfg] for u, (_, cfg, _, _) in zip(units, jobs))
     return {"metric": "serving: aggregate fitness evals/s (indiv x atoms), 32 concurrent jobs", "value": st["evals_per_s"],
-            "unit": UNIT, "n_gpus": 1, "jobs": len(jobs), "generations_per_job": gens, "status": rc,
-            "latency_ms": {"p50": st["p50_gen_ms"], "p99": st["p99_gen_ms"]}, "wall_s": wall,
+            "unit": UNIT, "n_gpus": 1, "jobs": len(jobs),
+            "generations_per_job": (f"until cancelled {args.serving_seconds:g} s after the last arrival" if steady
+                                    else gens),
+            "generations_done": {"min": int(min(done)), "max": int(max(done)), "total": int(sum(done))},
+            "status": rc if not steady else "cancelled after the steady-state period",
+            "latency_ms": {"device_p50": st["p50_gen_ms"], "device_p99": st["p99_gen_ms"],
+                           "wall_p50": st["p50_wall_gen_ms"], "wall_p99": st["p99_wall_gen_ms"]},
+            "wall_s": wall, "busy_s": st["busy_s"],
             "peak_resident_jobs": st["peak_resident_jobs"], "generation_batches": st["batches"],
             "total_units": total_units, "arrivals": "Poisson, 2 jobs/s",
             "one_at_a_time_plain_fp64_s_estimate": serial_plain_s,
-            # wall time includes the Poisson arrival gaps (about 16 s for 32 jobs at 2 jobs/s)
             "speedup_vs_one_at_a_time_plain_fp64": serial_plain_s / max(wall, 1e-9),
-            "busy_s": total_units / max(st["evals_per_s"], 1e-9),
-            "speedup_busy_vs_one_at_a_time_plain_fp64": serial_plain_s * st["evals_per_s"] / max(total_units, 1),
+            "speedup_busy_vs_one_at_a_time_plain_fp64": serial_plain_s / max(st["busy_s"], 1e-9),
             "data": "synthetic (workloads 1-3, 20-500 configurations, teacher targets)"}
 
 

@@ -88,7 +88,8 @@ PROTOTYPES = {
     "gpuga_server_result": (i32, [vp, i32, vp, vp]),
     "gpuga_server_cancel": (i32, [vp, i32]),
     "gpuga_server_drain": (i32, [vp, C.c_double]),
-    "gpuga_server_stats": (i32, [vp, vp]),
+    "gpuga_server_stats": (i32, [vp, vp, i32]),
+    "gpuga_server_hold": (i32, [vp, i32]),
     "gpuga_server_destroy": (i32, [vp]),
 }
 

@@ -33,6 +33,7 @@
 #include <cuda_pipeline.h>
 
 #include "engine.hpp"
+#include "exp_d.cuh"
 #include "powf_dd.cuh"
 
 namespace gpuga {
@@ -48,19 +49,22 @@ enum { TC_LR = 0, TC_LA = 2, TC_CR = 4, TC_CA = 6, TC_R0 = 8, TC_EN = 10, TC_BET
        TC_MHON, TC_LRL, TC_LAL = TC_LRL + 2, TC_CRL = TC_LAL + 2, TC_CAL = TC_CRL + 2, TC_MHONL = TC_CAL + 2,
        TC_COUNT };
 static_assert(TC_COUNT <= kMaxConsts, "per-individual Tersoff constants");
-// RI (ri.cu:36-110): qq[3], a[3], b[3] = 1/rho, c[3], rc, v_rc, dv_rc, Morse lr, la, cr, ca, r0,
-// then the FP64 remainders of b[3], lr and la (their FP32 roundings would otherwise shift the
-// exponents |d/rho|, |lr (d - r0)| of up to ~20 by 2^-24 relative), and the self-energy
-// coefficient K_C q^2 S(rc) as an FP32 pair (hi, lo) so that the energy items rebuild it in FP64.
-enum { RC_QQ = 0, RC_A = 3, RC_B = 6, RC_C = 9, RC_RC = 12, RC_VRC, RC_DVRC, RC_LR, RC_LA, RC_CR, RC_CA, RC_R0,
-       RC_BLO, RC_LRLO = RC_BLO + 3, RC_LALO, RC_SELF, RC_SELFLO, RC_COUNT };
+// RI (ri.cu:36-110), pair-by-pair part in FP32: Buckingham A[3], b[3] = 1/rho and its FP64
+// remainder (the exponent d/rho reaches ~20, where the FP32 rounding of b alone would move
+// e^{-d/rho} by ~1e-6), the cation-anion Morse constants lr, la (with remainders), cr, ca (with
+// remainders) and r0.  The linear part (damped shifted Coulomb and dispersion) takes FP64
+// constants: qq[3] (K_C included), C[3], v_rc, dv_rc, rc and the self-energy coefficient.
+enum { RC_A = 0, RC_B = 3, RC_BLO = 6, RC_LR = 9, RC_LA, RC_LRLO, RC_LALO, RC_CR, RC_CA, RC_CRLO, RC_CALO, RC_R0,
+       RC_COUNT };
 static_assert(RC_COUNT <= kMaxConsts, "per-individual RI constants");
+enum { R64_QQ = 0, R64_C = 3, R64_VRC = 6, R64_DVRC, R64_RC, R64_SELF, R64_COUNT };
 
 int consts_per_individual(const DevSet& d) {
   if (d.potential_type == 1 || d.potential_type == 2) return TC_COUNT;
   if (is_ri_type(d.potential_type)) return RC_COUNT;
   return 1;
 }
+int consts64_per_individual(const DevSet& d) { return is_ri_type(d.potential_type) ? R64_COUNT : 0; }
 
 __device__ __forceinline__ float decode1(float mn, float mx, float x) {
   return __fadd_rn(mn, __fmul_rn(__fsub_rn(mx, mn), x));  // fitness.cu:320-324, no contraction
@@ -108,23 +112,23 @@ __global__ void decode_jobs(const JobView* __restrict__ jobs, const int2* __rest
     put(TC_MHON, -0.5 / en);
     put_lo(TC_MHONL, -0.5 / en);
   } else if (is_ri_type(potential_type)) {
+    double* __restrict__ c64 = J.consts64;
+    auto put64 = [&](int k, double v) { c64[(size_t)k * Pstride + p] = v; };
     const double q0 = par(0), ratio = ri_charge_ratio(potential_type);
     const double kc = 14.399645;  // ri.cu:29
-    put(RC_QQ + 0, q0 * q0 * kc);
-    put(RC_QQ + 1, ratio * q0 * q0 * kc);
-    put(RC_QQ + 2, ratio * ratio * q0 * q0 * kc);
+    put64(R64_QQ + 0, q0 * q0 * kc);
+    put64(R64_QQ + 1, ratio * q0 * q0 * kc);
+    put64(R64_QQ + 2, ratio * ratio * q0 * q0 * kc);
     for (int t = 0; t < 3; ++t) {
       put(RC_A + t, par(1 + 3 * t));
       put(RC_B + t, 1.0 / par(2 + 3 * t));
       put_lo(RC_BLO + t, 1.0 / par(2 + 3 * t));
-      put(RC_C + t, par(3 + 3 * t));
+      put64(R64_C + t, par(3 + 3 * t));
     }
     const double rc = par(10), alpha = 0.2, pif = 0.225675833419103;
-    const double v_rc = erfc(alpha * rc) / rc;
-    const double dv_rc = -erfc(alpha * rc) / (rc * rc) - pif * exp(-alpha * alpha * rc * rc) / rc;
-    put(RC_RC, rc);
-    put(RC_VRC, J.ri_fixed_rc ? 0.0 : v_rc);  // a common cutoff is folded into the bond terms
-    put(RC_DVRC, J.ri_fixed_rc ? 0.0 : dv_rc);
+    put64(R64_VRC, erfc(alpha * rc) / rc);
+    put64(R64_DVRC, -erfc(alpha * rc) / (rc * rc) - pif * exp(-alpha * alpha * rc * rc) / rc);
+    put64(R64_RC, rc);
     const double d0 = par(11), al = par(12), r0 = par(13), s = par(14);
     put(RC_LR, sqrt(2.0 * s) * al);
     put(RC_LA, sqrt(2.0 / s) * al);
@@ -132,14 +136,14 @@ __global__ void decode_jobs(const JobView* __restrict__ jobs, const int2* __rest
     put_lo(RC_LALO, sqrt(2.0 / s) * al);
     put(RC_CR, d0 / (s - 1.0));
     put(RC_CA, s * d0 / (s - 1.0));
+    put_lo(RC_CRLO, d0 / (s - 1.0));
+    put_lo(RC_CALO, s * d0 / (s - 1.0));
     put(RC_R0, r0);
     // damped-Coulomb self energy per unit (q_i / q)^2 (develop/hfo2/find_E.m:10-13)
-    const double self = J.ri_self ? q0 * q0 * kc *
-                                        (alpha / sqrt(M_PI) + erfc(alpha * rc) / rc +
-                                         0.5 * pif * exp(-alpha * alpha * rc * rc))
-                                  : 0.0;
-    put(RC_SELF, self);
-    put_lo(RC_SELFLO, self);
+    put64(R64_SELF, J.ri_self ? q0 * q0 * kc *
+                                    (alpha / sqrt(M_PI) + erfc(alpha * rc) / rc +
+                                     0.5 * pif * exp(-alpha * alpha * rc * rc))
+                              : 0.0);
   } else {
     for (int m = 0; m < nv; ++m) weights[(size_t)m * Pstride + p] = decode1(pmin[m], pmax[m], x[m]);
   }
@@ -153,27 +157,45 @@ struct Consts {
 };
 
 // --------------------------------------------------------------------------- Tersoff
+// The lane's Tersoff constants.  The pair terms fr = cr e^{-lr t}, fa = ca e^{-la t} come in two
+// forms (tersoff_atom, PM): FP64 with FP64 constants (the FP32 value plus its FP64 remainder), or
+// FP32 with the remainders applied as first-order corrections.  The remainders are exactly zero
+// when S = 2, where the constants are FP32 parameters times powers of two.
+// Pair-term forms of the Tersoff items (tersoff_atom).
+enum PairMode { kPair32 = 0, kPair64 = 1 };
+
 struct TersoffC {
-  float lr[2], la[2], cr[2], ca[2], r0[2];
-  float lrl[2], lal[2], crl[2], cal[2];  // FP64 remainders of lr, la, cr, ca
+  double cr64[2], ca64[2], lr64[2], la64[2], r064[2];
+  float cr[2], ca[2], lr[2], la[2], r0[2], crl[2], cal[2], lrl[2], lal[2];
   float en, beta, h, r1, r2, pf, mhon, mhonl;
 };
 
-// LO: also load the FP64 remainders of lr, la, cr, ca (the remainder of -1/(2n) always).
-template <bool LO>
+// LO: the derived constants carry FP64 remainders (S not fixed at 2); PM: pair-term form (PairMode).
+template <bool LO, int PM>
 __device__ __forceinline__ void load_tersoff(const Consts& k, TersoffC& C) {
+  auto wide = [&](int hi, int lo) { return LO ? (double)k[hi] + (double)k[lo] : (double)k[hi]; };
 #pragma unroll
   for (int s = 0; s < 2; ++s) {
-    C.lr[s] = k[TC_LR + s];
-    C.la[s] = k[TC_LA + s];
-    C.cr[s] = k[TC_CR + s];
-    C.ca[s] = k[TC_CA + s];
-    C.r0[s] = k[TC_R0 + s];
-    if (LO) {
-      C.lrl[s] = k[TC_LRL + s];
-      C.lal[s] = k[TC_LAL + s];
-      C.crl[s] = k[TC_CRL + s];
-      C.cal[s] = k[TC_CAL + s];
+    if (PM == kPair64) {
+      C.ca64[s] = wide(TC_CA + s, TC_CAL + s);
+      C.la64[s] = wide(TC_LA + s, TC_LAL + s);
+      C.r064[s] = (double)k[TC_R0 + s];
+      if (LO) {  // S = 2: cr = ca / 2 and lr = 2 la, not needed
+        C.cr64[s] = wide(TC_CR + s, TC_CRL + s);
+        C.lr64[s] = wide(TC_LR + s, TC_LRL + s);
+      }
+    } else {
+      C.ca[s] = k[TC_CA + s];
+      C.la[s] = k[TC_LA + s];
+      C.r0[s] = k[TC_R0 + s];
+      C.cr[s] = k[TC_CR + s];
+      C.lr[s] = k[TC_LR + s];
+      if (LO) {
+        C.crl[s] = k[TC_CRL + s];
+        C.cal[s] = k[TC_CAL + s];
+        C.lrl[s] = k[TC_LRL + s];
+        C.lal[s] = k[TC_LAL + s];
+      }
     }
   }
   C.en = k[TC_EN];
@@ -256,6 +278,8 @@ __device__ __forceinline__ void reduce_item(const WorkItem& it, int P, int Nc, d
 template <int ST>
 struct GeoT {
   const float4* g;     // (unit vector, d)
+  const double* d64;   // d in FP64
+  const float* dlo;    // d - (float)d
   const uint8_t* pt;   // pair set
   const int* rev;      // slot * Na + atom of the reverse bond (force scratch position)
   const int* nn;       // [Na]
@@ -277,11 +301,14 @@ using Geo = GeoT<-1>;
 
 // Copies configuration c's geometry into shared memory, slot-major with ZC
 // slots, with all threads of the CTA (independent loads, then one barrier).
-template <int ZC>
+// D64: the FP64 bond lengths (FP64 pair terms), else their FP32 remainders.
+template <int ZC, bool D64>
 __device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int Na, bool force, unsigned char* base) {
   const int n = ZC * Na;
   float4* sg = reinterpret_cast<float4*>(base);
-  int* snn = reinterpret_cast<int*>(sg + n);
+  double* sd = reinterpret_cast<double*>(sg + n);
+  float* sl = reinterpret_cast<float*>(sd + (D64 ? n : 0));
+  int* snn = reinterpret_cast<int*>(sl + (D64 ? 0 : n));
   int* srev = snn + Na;
   uint8_t* spt = reinterpret_cast<uint8_t*>(srev + (force ? n : 0));
   for (int t = threadIdx.x; t < n; t += blockDim.x) {
@@ -289,17 +316,19 @@ __device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int N
     if (j < S.NN[i]) {
       const int b = S.off[i] + j;
       sg[t] = __ldg(&S.g32[b]);
+      if (D64) sd[t] = __ldg(&S.d64[b]);
+      else sl[t] = __ldg(&S.tdl[b]);
       spt[t] = S.ptype[b];
       if (force) srev[t] = S.rev_sm[b];
     }
   }
   for (int k = threadIdx.x; k < Na; k += blockDim.x) snn[k] = S.NN[atom0 + k];
   __syncthreads();
-  return Geo{sg, spt, srev, snn, nullptr, 0, Na};
+  return Geo{sg, sd, sl, spt, srev, snn, nullptr, 0, Na};
 }
 
 // One atom of the minimal Tersoff potential (minimal_tersoff.cu:122-405) for
-// the lane's parameter vector.  Returns the site energy; writes the partial
+// the lane's parameter vector.  Returns the site energy (FP64); writes the partial
 // forces f_ij (FORCE) or adds -r_ij (x) f_ij into v[6] (energy/virial items).
 //
 // With unit vectors u and the bond scalars
@@ -308,11 +337,19 @@ __device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int N
 //   f_ij = 1/2 [ (A'_j - fc'_j sum_k T_k g_jk - m_j sum_k q_jk cos_jk) u_j + m_j sum_k q_jk u_k ]
 // with q_jk = beta (cos_jk - h) (S_j fc_k + T_k) and m_j = -2 fc_j / d_j.
 //
+// Precision.  Near equilibrium fr - b fa and fr' - b fa' are small differences of large
+// terms, and the virial sums the radial forces of thousands of bonds, so the pair terms are
+// evaluated in FP64 (FP64 bond length and constants, FP64 exponentials exp_d.cuh; when S = 2,
+// lr = 2 la and one exponential serves both terms): the site energy and A'_j are rounded once, after the
+// cancellation.  Measured on the 500-configuration Si set, this took the relative fitness error
+// of individuals near the fitted optimum from 8.5e-7 to 2.4e-7; the bond order and the
+// three-body terms stay FP32 (b to ~1 ulp, powf_dd.cuh).
+//
 // FULL: every one of the ZC bond slots is present (Z == ZC, e.g. all atoms of a diamond
 // lattice), so that the per-slot guards fold away at compile time.
-template <int ZC, int NT, bool FORCE, bool FULL, bool LO, class GEO>
-__device__ __forceinline__ float tersoff_atom(const GEO& geo, const TersoffC& C, int il, int Na, float* fsm, int G,
-                                              int g, float (&v)[6]) {
+template <int ZC, int NT, bool FORCE, bool FULL, bool LO, int PM, class GEO>
+__device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C, int il, int Na, float* fsm, int G,
+                                               int g, float (&v)[6]) {
   const int Z = FULL ? ZC : geo.nn[il];
   const int b0 = geo.base(il), bs = geo.step();  // bond j at b0 + j * bs
   float ux[ZC], uy[ZC], uz[ZC], dd[ZC];
@@ -332,26 +369,12 @@ __device__ __forceinline__ float tersoff_atom(const GEO& geo, const TersoffC& C,
       dd[j] = 1.0f;
     }
   }
-  // pass A: pair terms and cutoff of every bond
-  float fc[ZC], fcp[ZC], fr[ZC], fa[ZC];
+  // pass A: cutoff of every bond
+  float fc[ZC], fcp[ZC];
 #pragma unroll
   for (int j = 0; j < ZC; ++j) {
-    fc[j] = fcp[j] = fr[j] = fa[j] = 0.f;
-    if (j < Z) {
-      const int s = NT == 2 ? st[j] : 0;
-      const float t = dd[j] - (s ? C.r0[1] : C.r0[0]);
-      const float cr = s ? C.cr[1] : C.cr[0], ca = s ? C.ca[1] : C.ca[0];
-      const float er = expf(-(s ? C.lr[1] : C.lr[0]) * t), ea = expf(-(s ? C.la[1] : C.la[0]) * t);
-      if constexpr (LO) {
-        // c e^{-l t} with c = c_h + c_l, l = l_h + l_l:  c_h E + (c_l - c_h l_l t) E, E = e^{-l_h t}
-        fr[j] = fmaf(fmaf(-cr * (s ? C.lrl[1] : C.lrl[0]), t, s ? C.crl[1] : C.crl[0]), er, cr * er);
-        fa[j] = fmaf(fmaf(-ca * (s ? C.lal[1] : C.lal[0]), t, s ? C.cal[1] : C.cal[0]), ea, ca * ea);
-      } else {
-        fr[j] = cr * er;
-        fa[j] = ca * ea;
-      }
-      cutoff_fn(C.r1, C.r2, C.pf, dd[j], fc[j], fcp[j]);
-    }
+    fc[j] = fcp[j] = 0.f;
+    if (j < Z) cutoff_fn(C.r1, C.r2, C.pf, dd[j], fc[j], fcp[j]);
   }
   // pass B: bond order, site energy and the per-bond force scalars
   // cos(theta_jik) = u_j . u_k from the FP32 unit vectors (as accurate as a stored FP32 cosine);
@@ -371,7 +394,8 @@ __device__ __forceinline__ float tersoff_atom(const GEO& geo, const TersoffC& C,
     else return fmaf(uz[j], uz[k], fmaf(uy[j], uy[k], ux[j] * ux[k]));
   };
   float Ap[ZC], Sb[ZC], Tb[ZC];
-  float pe = 0.f;
+  double pe = 0.0;    // FP64 pair terms
+  float pe32 = 0.f;   // FP32 pair terms
 #pragma unroll
   for (int j = 0; j < ZC; ++j) {
     Ap[j] = Sb[j] = Tb[j] = 0.f;
@@ -391,16 +415,53 @@ __device__ __forceinline__ float tersoff_atom(const GEO& geo, const TersoffC& C,
         b = powf_dd(opz, C.mhon, C.mhonl);
         bp = __fdividef(-0.5f * b * zn, opz * zeta);
       }
+      // pair terms fr = cr e^{-lr t}, fa = ca e^{-la t}, t = d - r0.  With S = 2 (!LO) lr = 2 la
+      // and cr = ca / 2, so fr = fa e^{-la t} / 2 from the one exponential.
       const int s = NT == 2 ? st[j] : 0;
-      const float e = fr[j] - b * fa[j];
-      pe = fmaf(0.5f * fc[j], e, pe);
-      float frp = -(s ? C.lr[1] : C.lr[0]) * fr[j], fap = -(s ? C.la[1] : C.la[0]) * fa[j];
-      if constexpr (LO) {
-        frp = fmaf(-(s ? C.lrl[1] : C.lrl[0]), fr[j], frp);
-        fap = fmaf(-(s ? C.lal[1] : C.lal[0]), fa[j], fap);
+      float fa32;
+      if constexpr (PM == kPair64) {
+        const double t = geo.d64[b0 + j * bs] - (s ? C.r064[1] : C.r064[0]);
+        const double la = s ? C.la64[1] : C.la64[0];
+        const double ea = exp_d<10>(-la * t);
+        const double fa = (s ? C.ca64[1] : C.ca64[0]) * ea;
+        const double fr = LO ? (s ? C.cr64[1] : C.cr64[0]) * exp_d<10>(-(s ? C.lr64[1] : C.lr64[0]) * t)
+                             : 0.5 * fa * ea;
+        const double lr_fr = LO ? (s ? C.lr64[1] : C.lr64[0]) * fr : 2.0 * la * fr;
+        const double bd = b;
+        const double e = fr - bd * fa;
+        if (fc[j] == 1.0f && fcp[j] == 0.0f) {  // inside r1: no conversions of fc, fc'
+          pe = fma(0.5, e, pe);
+          Ap[j] = (float)fma(bd * la, fa, -lr_fr);
+        } else {
+          pe = fma(0.5 * (double)fc[j], e, pe);
+          Ap[j] = (float)fma((double)fcp[j], e, (double)fc[j] * fma(bd * la, fa, -lr_fr));
+        }
+        fa32 = (float)fa;
+      } else {
+        // FP32: two exponentials (for a lattice's narrow range of bond lengths their rounding
+        // errors are alike and cancel in fr' - b fa'), the FP64 remainder of d as a first-order
+        // correction e^{-l (t + d_lo)} = e^{-l t} (1 - l d_lo), and for S != 2 the remainders of
+        // the constants c e^{-l t} = c_h E + (c_l - c_h l_l t) E, l f = l_h f + l_l f
+        const float t = dd[j] - (s ? C.r0[1] : C.r0[0]), dlo = geo.dlo[b0 + j * bs];
+        const float lr = s ? C.lr[1] : C.lr[0], la = s ? C.la[1] : C.la[0];
+        const float cr = s ? C.cr[1] : C.cr[0], ca = s ? C.ca[1] : C.ca[0];
+        float er = expf(-lr * t), ea = expf(-la * t);
+        er = fmaf(-lr * dlo, er, er);
+        ea = fmaf(-la * dlo, ea, ea);
+        float fr = cr * er, fa = ca * ea;
+        float frp = -lr * fr, fap = -la * fa;
+        if constexpr (LO) {
+          fr = fmaf(fmaf(-cr * (s ? C.lrl[1] : C.lrl[0]), t, s ? C.crl[1] : C.crl[0]), er, fr);
+          fa = fmaf(fmaf(-ca * (s ? C.lal[1] : C.lal[0]), t, s ? C.cal[1] : C.cal[0]), ea, fa);
+          frp = fmaf(-(s ? C.lrl[1] : C.lrl[0]), fr, -lr * fr);
+          fap = fmaf(-(s ? C.lal[1] : C.lal[0]), fa, -la * fa);
+        }
+        const float e = fr - b * fa;
+        pe32 = fmaf(0.5f * fc[j], e, pe32);
+        Ap[j] = fcp[j] * e + fc[j] * (frp - b * fap);
+        fa32 = fa;
       }
-      Ap[j] = fcp[j] * e + fc[j] * (frp - b * fap);
-      Sb[j] = bp * fa[j];
+      Sb[j] = bp * fa32;
       Tb[j] = Sb[j] * fc[j];
     }
   }
@@ -448,7 +509,7 @@ __device__ __forceinline__ float tersoff_atom(const GEO& geo, const TersoffC& C,
       }
     }
   }
-  return pe;
+  return pe + (double)pe32;
 }
 
 // Energy/virial items (FORCE = false) keep their FP64 per-lane sums in shared
@@ -458,10 +519,19 @@ __device__ __forceinline__ float tersoff_atom(const GEO& geo, const TersoffC& C,
 // GT: the item's individuals per item G as a compile-time constant (0: read from the item), so
 // that the force scratch addressing and the atom-slot split fold into shifts and constants;
 // ST: staged (1) or in-place CSR (0) geometry, or decided per item (-1).
+// Pair-term form of the two kinds of Tersoff items (tersoff_atom, PairMode).  Energy/virial items
+// take the FP64 pair terms: the configuration virial sums the radial forces of all bonds, whose
+// cancellation near equilibrium amplifies FP32 rounding.  Force items stay FP32: their force error
+// was the same with FP64 pair terms (500-configuration Si set, individuals near the optimum: 2.2e-7
+// vs 2.3e-7 of the force RMSE) at 40 % more time.
+constexpr int kPairModeEV = kPair64;
+constexpr int kPairModeForce = kPair32;
+
 template <int ZC, int NT, bool FORCE, int BLK, int GT, int ST, bool LO>
 __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, const WorkItem& it,
                                              unsigned char* smem) {
   constexpr int NW = BLK / 32;
+  constexpr int PM = FORCE ? kPairModeForce : kPairModeEV;
   const JobView& J = jobs[it.job];
   const DevView S = J.v;
   const int P = J.P;
@@ -473,7 +543,7 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
   const int p = it.p0 + g;
   const Consts kc{J.consts, J.Pstride, p < P ? p : it.p0};
   TersoffC C;
-  load_tersoff<LO>(kc, C);
+  load_tersoff<LO, PM>(kc, C);
   const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
   const int bond0 = S.off[atom0];
   // force scratch: shared memory, or for configurations too large for it the item's own
@@ -487,10 +557,11 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
   }
   GeoT<ST> geo;
   if (ST == 1 || (ST == -1 && item_staged(it))) {
-    const Geo s0 = stage_geometry<ZC>(S, atom0, Na, FORCE, smem + front);
-    geo = GeoT<ST>{s0.g, s0.pt, s0.rev, s0.nn, s0.boff, s0.bond0, s0.stride};
+    const Geo s0 = stage_geometry<ZC, PM == kPair64>(S, atom0, Na, FORCE, smem + front);
+    geo = GeoT<ST>{s0.g, s0.d64, s0.dlo, s0.pt, s0.rev, s0.nn, s0.boff, s0.bond0, s0.stride};
   } else {
-    geo = GeoT<ST>{S.g32 + bond0, S.ptype + bond0, S.rev_sm + bond0, S.NN + atom0, S.off + atom0, bond0, 0};
+    geo = GeoT<ST>{S.g32 + bond0, S.d64 + bond0, S.tdl + bond0, S.ptype + bond0, S.rev_sm + bond0, S.NN + atom0,
+                   S.off + atom0, bond0, 0};
   }
   for (int base = warp * A; base < Na; base += NW * A) {
     const int il = base + aslot;
@@ -498,10 +569,10 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
     const bool full = __all_sync(0xffffffffu, il >= Na || geo.nn[il] == ZC);
     if (il < Na) {
       float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      const float pe = full ? tersoff_atom<ZC, NT, FORCE, true, LO>(geo, C, il, Na, fsm, G, g, v)
-                            : tersoff_atom<ZC, NT, FORCE, false, LO>(geo, C, il, Na, fsm, G, g, v);
+      const double pe = full ? tersoff_atom<ZC, NT, FORCE, true, LO, PM>(geo, C, il, Na, fsm, G, g, v)
+                            : tersoff_atom<ZC, NT, FORCE, false, LO, PM>(geo, C, il, Na, fsm, G, g, v);
       if (!FORCE) {
-        red[threadIdx.x] += (double)pe;
+        red[threadIdx.x] += pe;
 #pragma unroll
         for (int k = 0; k < 6; ++k) red[(k + 1) * BLK + threadIdx.x] += (double)v[k];
       }
@@ -587,37 +658,34 @@ __global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_ba
 }
 
 // --------------------------------------------------------------------------- RI / NN2B
-// RI pair term (ri.cu:77-110) with the geometry-only Coulomb pieces precomputed:
-// gri = (d - (float)d, 1/d^6, erfc(alpha d)/d, erfc(alpha d)/d^2 + 2 alpha/sqrt(pi) exp(-alpha^2 d^2)/d).
-// Returns U(d) in p2 and dU/dd in fd.
+// RI pair by pair (ri.cu:77-110): only the terms that are not linear in the per-individual
+// constants, the Buckingham repulsion A e^{-d/rho} and, for cation-anion pairs, the Morse pair
+// cr e^{-lr (d - r0)} - ca e^{-la (d - r0)}.  The damped shifted Coulomb and the dispersion
+// -C/d^6 enter through their FP64 geometric sums (ri_linear_atoms, geometry.cu), so the large
+// alternating Coulomb terms never pass through FP32 arithmetic.
 //
-// The exponents d/rho (Buckingham) and lr (d - r0), la (d - r0) (Morse) reach
-// ~20, so their FP32 rounding alone would move exp() by ~1e-6 relative; they
-// are formed as hi + lo (exact FMA residuals, the FP64 remainders of d, 1/rho,
-// lr and la) and exp(-(hi + lo)) = exp(-hi) (1 - lo).
+// The exponents d/rho and lr (d - r0), la (d - r0) reach ~20, so their FP32 rounding alone
+// would move exp() by ~1e-6 relative; they are formed as hi + lo (exact FMA residuals, the FP64
+// remainders of d, 1/rho, lr and la) and exp(-(hi + lo)) = exp(-hi) (1 - lo).
 struct RIC {  // the lane's RI constants, loaded once per work item
-  float qq[3], a[3], b[3], blo[3], c6[3], c[3], rc, vrc, dvrc, lr, la, lrlo, lalo, cr, ca, r0;
+  float a[3], b[3], blo[3], lr, la, lrlo, lalo, cr, ca, crlo, calo, r0;
 };
 
 __device__ __forceinline__ void load_ri(const Consts& k, RIC& R) {
 #pragma unroll
   for (int t = 0; t < 3; ++t) {
-    R.qq[t] = k[RC_QQ + t];
     R.a[t] = k[RC_A + t];
     R.b[t] = k[RC_B + t];
     R.blo[t] = k[RC_BLO + t];
-    R.c[t] = k[RC_C + t];
-    R.c6[t] = 6.0f * R.c[t];
   }
-  R.rc = k[RC_RC];
-  R.vrc = k[RC_VRC];
-  R.dvrc = k[RC_DVRC];
   R.lr = k[RC_LR];
   R.la = k[RC_LA];
   R.lrlo = k[RC_LRLO];
   R.lalo = k[RC_LALO];
   R.cr = k[RC_CR];
   R.ca = k[RC_CA];
+  R.crlo = k[RC_CRLO];
+  R.calo = k[RC_CALO];
   R.r0 = k[RC_R0];
 }
 
@@ -631,27 +699,60 @@ __device__ __forceinline__ float exp_neg_dd(float xh, float xl, float yh, float 
 
 // Pair type T (0 cation-cation, 1 cation-anion with Morse, 2 anion-anion) at compile time:
 // the lane's constants of that type stay in registers and the Morse terms exist only for T = 1.
+// Returns the pair energy in p2 and dU/dd in fd.
 template <int T>
-__device__ __forceinline__ void ri_pair(const RIC& R, float d, float4 w, float& p2, float& fd) {
-  const float dlo = w.x;
-  const float ex = exp_neg_dd(d, dlo, R.b[T], R.blo[T]);
-  p2 = R.a[T] * ex - R.c[T] * w.y + R.qq[T] * (w.z - R.vrc - R.dvrc * (d - R.rc));
-  fd = __fdividef(R.c6[T] * w.y, d) - R.a[T] * ex * R.b[T] - R.qq[T] * (w.w + R.dvrc);
+__device__ __forceinline__ void ri_pair(const RIC& R, float d, float dlo, float& p2, float& fd) {
+  const float ex = R.a[T] * exp_neg_dd(d, dlo, R.b[T], R.blo[T]);
+  p2 = ex;
+  fd = -fmaf(ex, R.b[T], ex * R.blo[T]);
   if constexpr (T == 1) {
     // d - r0 as hi + lo (TwoSum), then the two Morse exponentials
     const float drh = d - R.r0;
     const float bb = drh - d;
     const float drl = ((d - (drh - bb)) + (-R.r0 - bb)) + dlo;
-    const float fr = R.cr * exp_neg_dd(drh, drl, R.lr, R.lrlo);
-    const float fa = R.ca * exp_neg_dd(drh, drl, R.la, R.lalo);
+    const float er = exp_neg_dd(drh, drl, R.lr, R.lrlo), ea = exp_neg_dd(drh, drl, R.la, R.lalo);
+    const float fr = fmaf(R.crlo, er, R.cr * er), fa = fmaf(R.calo, ea, R.ca * ea);
     p2 += fr - fa;
-    fd += -R.lr * fr + R.la * fa;
+    fd += fmaf(R.la, fa, R.lalo * fa) - fmaf(R.lr, fr, R.lrlo * fr);
+  }
+}
+
+// FP64 linear part of one (individual, energy/virial configuration): energy and virial from the
+// configuration's geometric sums g[kRiCfgLin] (per pair type t: sum ec, count, sum d, sum 1/d^6,
+// then sum d gc uu, sum d uu, sum uu / d^6) and the lane's FP64 constants.
+__device__ __forceinline__ void ri_linear_config(const double* __restrict__ g, const double* __restrict__ c64,
+                                                 int stride, double (&acc)[kResK]) {
+  const double vrc = c64[R64_VRC * (size_t)stride], dvrc = c64[R64_DVRC * (size_t)stride],
+               rc = c64[R64_RC * (size_t)stride];
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    const double qq = c64[(R64_QQ + t) * (size_t)stride], C = c64[(R64_C + t) * (size_t)stride];
+    const double* gt = g + 22 * t;
+    // U_lin = qq ec + qq (dv_rc rc - v_rc) - qq dv_rc d - C / d^6
+    acc[0] += qq * gt[0] + qq * (dvrc * rc - vrc) * gt[1] - qq * dvrc * gt[2] - C * gt[3];
+    // W = -sum d dU/dd uu with dU/dd = -qq (gc + dv_rc) + 6 C / d^7
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[1 + k] += qq * gt[4 + k] + qq * dvrc * gt[10 + k] - 6.0 * C * gt[16 + k];
+  }
+}
+
+// FP64 linear part of the force on one atom: F_i = sum_t [-qq_t (sum gc u + dv_rc sum u) + 6 C_t sum u / d^7].
+__device__ __forceinline__ void ri_linear_force(const double* __restrict__ g, const double* __restrict__ c64,
+                                                int stride, double (&F)[3]) {
+  const double dvrc = c64[R64_DVRC * (size_t)stride];
+  F[0] = F[1] = F[2] = 0.0;
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    const double qq = c64[(R64_QQ + t) * (size_t)stride], C = c64[(R64_C + t) * (size_t)stride];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) F[a] += -qq * (g[9 * t + a] + dvrc * g[9 * t + 3 + a]) + 6.0 * C * g[9 * t + 6 + a];
   }
 }
 
 // bonds per chunk of the RI pair pipeline (one bond per lane); two stages per warp
 constexpr int kPairChunk = 32;
-constexpr size_t kPairStageBytes = (size_t)kWarps * 2 * 2 * kPairChunk * sizeof(float4);
+constexpr size_t kPairStageOne = (size_t)kPairChunk * (sizeof(float4) + sizeof(float));  // geometry | d lo
+constexpr size_t kPairStageBytes = (size_t)kWarps * 2 * kPairStageOne;
 
 // Compensated FP32 sum (Kahan): the running error c is subtracted from each
 // new term; value() is the sum in FP64.  Error about 2 eps sum|x| for any
@@ -796,20 +897,39 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
   double acc[kResK];
 #pragma unroll
   for (int k = 0; k < kResK; ++k) acc[k] = 0.0;
-  // RI self energy: an energy item covers all atoms of its configuration, so warp 0 adds
-  // -K_C q^2 S sum_i (q_i / q)^2 once per individual, in FP64
-  if (KIND == 1 && !FORCE && J.ri_self && warp == 0)
-    acc[0] = -((double)kc[RC_SELF] + (double)kc[RC_SELFLO]) * S.ri_qsum[c];
+  // RI energy/virial items cover all atoms of their configuration, so warp 0 adds the linear
+  // part (Coulomb, dispersion) and the self energy -K_C q^2 S sum_i (q_i / q)^2 once per
+  // individual, in FP64
+  const double* __restrict__ c64 = KIND == 1 ? J.consts64 + pl : nullptr;
+  if (KIND == 1 && !FORCE && warp == 0) {
+    if (J.ri_self) acc[0] = -c64[R64_SELF * (size_t)Pstride] * S.ri_qsum[c];
+    ri_linear_config(S.ri_cfg_lin + (size_t)c * kRiCfgLin, c64, Pstride, acc);
+  }
   // per-atom sums over the atom's pairs in FP32, added to the FP64 accumulators once per atom
   // (a per-pair FP64 add would cost two FP32->FP64 conversions per term, which run at a
-  // fraction of the FP32 rate).  The energy is compensated (Kahan); the force and virial
-  // components are plain FMA sums: compensating them left the fitness error of 400 individuals
-  // unchanged (rigid-ion set: max 5.5e-7 / 5.8e-7, p99 2.2e-7 either way; NN2B identical) and
-  // cost 18 % of the rigid-ion generation (6.82 -> 5.69 ms).  The per-pair terms' own FP32
-  // errors, not the summation, set the error here.
+  // fraction of the FP32 rate).  The energy is compensated (Kahan).  For the rigid ion the force
+  // and virial components are compensated as well: once the Coulomb and dispersion terms moved to
+  // the FP64 linear part, the FP32 summation of the large nearest-neighbour Buckingham terms set
+  // the error of individuals near the fitted optimum (300-configuration set: max 1.5e-6 with FMA
+  // sums, 7.6e-7 compensated, for 16 % of the pair time).  NN2B keeps FMA sums (its error is set
+  // by the per-pair terms: compensation left it unchanged).
   constexpr int NK = FORCE ? 3 : 7;
   auto consume = [&](KSum* ks, const float4& q, float p2, float fd) {
-    if (FORCE) {
+    if (KIND == 1 && FORCE) {
+      ks[0].add(fd * q.x);
+      ks[1].add(fd * q.y);
+      ks[2].add(fd * q.z);
+    } else if (KIND == 1) {
+      ks[0].add(p2);
+      const float s = -q.w * fd;
+      const float sx = s * q.x, sy = s * q.y, sz = s * q.z;
+      ks[1].add(sx * q.x);
+      ks[2].add(sy * q.y);
+      ks[3].add(sz * q.z);
+      ks[4].add(sx * q.y);
+      ks[5].add(sy * q.z);
+      ks[6].add(sz * q.x);
+    } else if (FORCE) {
       ks[0].s = fmaf(fd, q.x, ks[0].s);
       ks[1].s = fmaf(fd, q.y, ks[1].s);
       ks[2].s = fmaf(fd, q.z, ks[2].s);
@@ -829,15 +949,19 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
   auto finish_atom = [&](int il, KSum* ks) {
     if (FORCE) {
       const int i = atom0 + il;
-      const double dx = ks[0].value() - (double)S.force_ref[i];
-      const double dy = ks[1].value() - (double)S.force_ref[i + N];
-      const double dz = ks[2].value() - (double)S.force_ref[i + 2 * (size_t)N];
+      double F[3] = {0.0, 0.0, 0.0};
+      if (KIND == 1) ri_linear_force(S.ri_atom_lin + (size_t)i * kRiAtomLin, c64, Pstride, F);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) F[a] += ks[a].value();
+      const double dx = F[0] - (double)S.force_ref[i];
+      const double dy = F[1] - (double)S.force_ref[i + N];
+      const double dz = F[2] - (double)S.force_ref[i + 2 * (size_t)N];
       acc[7] += dx * dx + dy * dy + dz * dz;
       if (fdump && p < P) {
         const int Nf = S.N_force;
-        fdump[((size_t)p * 3 + 0) * Nf + i] = (float)ks[0].value();
-        fdump[((size_t)p * 3 + 1) * Nf + i] = (float)ks[1].value();
-        fdump[((size_t)p * 3 + 2) * Nf + i] = (float)ks[2].value();
+        fdump[((size_t)p * 3 + 0) * Nf + i] = (float)F[0];
+        fdump[((size_t)p * 3 + 1) * Nf + i] = (float)F[1];
+        fdump[((size_t)p * 3 + 2) * Nf + i] = (float)F[2];
       }
     } else {
 #pragma unroll
@@ -858,8 +982,12 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
     // asynchronous copies (cp.async, 16 B per lane) bring the next one, so the L2 latency of the
     // per-bond geometry is hidden behind the pair arithmetic.  Every atom yields at least one
     // chunk (possibly empty: force items still owe the atom's force error).
-    float4* buf = reinterpret_cast<float4*>(smem + (size_t)kWarps * 32 * kResK * sizeof(double)) +
-                  (size_t)warp * 4 * kPairChunk;  // [stage][geometry | Coulomb terms][kPairChunk]
+    // [stage][geometry float4 | d lo float][kPairChunk]
+    unsigned char* buf = smem + (size_t)kWarps * 32 * kResK * sizeof(double) + (size_t)warp * 2 * kPairStageOne;
+    auto stage_g = [&](int st) { return reinterpret_cast<float4*>(buf + st * kPairStageOne); };
+    auto stage_dl = [&](int st) {
+      return reinterpret_cast<float*>(buf + st * kPairStageOne + kPairChunk * sizeof(float4));
+    };
     // the atom's pairs come grouped by pair type (rseg), so a chunk splits into at most three
     // runs of one type each, evaluated with that type's constants hoisted
     int4 f_seg = make_int4(0, 0, 0, 0);
@@ -889,8 +1017,8 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
       }
       if (lane < q_n[st]) {
         const int bnd = q_b[st] + lane;
-        __pipeline_memcpy_async(buf + (2 * st) * kPairChunk + lane, S.rg32 + bnd, sizeof(float4));
-        __pipeline_memcpy_async(buf + (2 * st + 1) * kPairChunk + lane, S.rgri + bnd, sizeof(float4));
+        __pipeline_memcpy_async(stage_g(st) + lane, S.rg32 + bnd, sizeof(float4));
+        __pipeline_memcpy_async(stage_dl(st) + lane, S.rdl + bnd, sizeof(float));
       }
     };
     fetch(0);
@@ -900,8 +1028,8 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
     for (int st = 0; q_has[st]; st ^= 1) {
       __pipeline_wait_prior(1);  // the older of the two groups in flight (stage st) has landed
       __syncwarp();
-      const float4* g = buf + (2 * st) * kPairChunk;
-      const float4* w = g + kPairChunk;
+      const float4* g = stage_g(st);
+      const float* w = stage_dl(st);
       const int n = q_n[st], b0 = q_b[st];
       const int k1 = min(max(q_s1[st] - b0, 0), n), k2 = min(max(q_s2[st] - b0, 0), n);
       auto run = [&](auto type, int kb, int ke) {
@@ -1042,9 +1170,13 @@ DevView make_view(const DevSet& d) {
   v.rev_sm = d.rev_sm;
   v.ptype = d.ptype;
   v.g32 = d.g32;
+  v.d64 = d.d64;
+  v.tdl = d.tdl;
   v.rg32 = d.rg32;
-  v.rgri = d.rgri;
+  v.rdl = d.rdl;
   v.rseg = d.rseg;
+  v.ri_atom_lin = d.ri_atom_lin;
+  v.ri_cfg_lin = d.ri_cfg_lin;
   v.force_ref = d.force_ref;
   v.ri_qsum = d.ri_qsum;
   return v;
@@ -1061,7 +1193,6 @@ JobView make_job_view(const Engine* e, const Plan* plan) {
   j.P = plan->P;
   j.Pstride = plan->Pstride;
   j.Nc_force = d.Nc_force;
-  j.ri_fixed_rc = d.ri_fixed_rc;
   j.ri_self = e->spec.ri_self;
   j.tp = NNTaper{e->spec.nn_r1, e->spec.nn_r2, (float)(M_PI / ((double)e->spec.nn_r2 - e->spec.nn_r1)),
                  e->spec.nn_consistent};
@@ -1069,6 +1200,7 @@ JobView make_job_view(const Engine* e, const Plan* plan) {
   j.pmin = e->d_pmin;
   j.pmax = e->d_pmax;
   j.consts = plan->d_consts;
+  j.consts64 = plan->d_consts64;
   j.weights = plan->d_weights;
   j.res = plan->d_res;
   j.fdump = plan->dump ? plan->d_fdump : nullptr;
@@ -1134,7 +1266,8 @@ static bool tersoff_consts_exact(const PotentialSpec& sp, int num_types) {
 //   Algorithmic work per (individual, atom), counted on the batched formulation
 //   (FMA = 2 flops; exp/pow/erfc/tanh/sin-cos calls counted as SFU work):
 //     Tersoff: 60 flops + 4 transcendentals per bond, 21 flops per ordered triplet
-//     RI:      25 flops + 2 transcendentals per pair (Morse included on average)
+//     RI:      per pair of an active type 20 flops + 1 exp, cation-anion pairs 20 more + 2 exp
+//              (Morse); the linear terms are FP64 sums formed once per training set
 //     NN2B:    4n^2 + 13n + 10 flops + 2n tanh per pair
 int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<ItemSpec>>& groups,
               std::map<LaunchKey, size_t>& smem_need, size_t* gscratch_floats) {
@@ -1156,10 +1289,28 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
     if (kind == 0) {
       atom_flops[i] = 60.0 * Z + 21.0 * Z * (Z - 1.0);
       atom_sfu[i] = 4.0 * Z;
+    } else if (kind == 1) {
+      // evaluated pairs only (ri_active), by pair type
+      double f = 0, sf = 0, fh = 0, sfh = 0;
+      for (int b = e->h_off[i]; b < e->h_off[i + 1]; ++b) {
+        const int t = ts.type[i] + ts.type[e->h_nbr[b]];
+        if (!((d.ri_active >> t) & 1)) continue;
+        const double pf = t == 1 ? 40.0 : 20.0, ps = t == 1 ? 3.0 : 1.0;
+        f += pf;
+        sf += ps;
+        if (e->h_nbr[b] > i) {
+          fh += pf;
+          sfh += ps;
+        }
+      }
+      atom_flops[i] = f;
+      atom_sfu[i] = sf;
+      atom_flops_half[i] = fh;
+      atom_sfu_half[i] = sfh;
     } else {
       const double nn = d.num_neurons;
-      const double fpp = kind == 1 ? 25.0 : 4.0 * nn * nn + 13.0 * nn + 10.0;
-      const double spp = kind == 1 ? 2.0 : 2.0 * nn;
+      const double fpp = 4.0 * nn * nn + 13.0 * nn + 10.0;
+      const double spp = 2.0 * nn;
       int half = 0;
       for (int b = e->h_off[i]; b < e->h_off[i + 1]; ++b) half += e->h_nbr[b] > i;
       atom_flops[i] = fpp * Z;
@@ -1183,8 +1334,11 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
                   e->h_zmax[c]);
         return GPUGA_ERR_UNSUPPORTED;
       }
-      // slot-major staged geometry: zc slots per atom of (float4, pair set[, reverse position]) + counts
-      const size_t stage = ((size_t)zc * Na * (16 + 1 + (force ? 4 : 0)) + (size_t)Na * 4 + 15) & ~(size_t)15;
+      // slot-major staged geometry: zc slots per atom of (float4, the FP64 length (FP64 pair terms)
+      // or its FP32 remainder, pair set[, reverse position]) + counts
+      const bool d64 = (force ? kPairModeForce : kPairModeEV) == kPair64;
+      const size_t stage =
+          ((size_t)zc * Na * (16 + (d64 ? 8 : 4) + 1 + (force ? 4 : 0)) + (size_t)Na * 4 + 15) & ~(size_t)15;
       const size_t per_ind = (size_t)e->h_zmax[c] * Na * 3 * sizeof(float);  // slot-major, padded to max Z
       if (force && per_ind > force_smem_target(zc)) {
         // not even one individual's scratch fits: 32 individuals per item (lane = individual,
@@ -1305,7 +1459,8 @@ int launch_one(const LaunchSet* ls, const Launch& L, cudaStream_t st, bool confi
 
 }  // namespace
 
-int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSet* ls) {
+int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSet* ls,
+                    const std::vector<std::pair<const float*, double*>>* targets) {
   std::map<LaunchKey, std::vector<ItemSpec>> groups;
   std::map<LaunchKey, size_t> smem_need;
   std::vector<int2> indmap;
@@ -1320,6 +1475,10 @@ int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSe
       plan->gscratch_floats = need;
     }
     ls->jobs.push_back(make_job_view(e, plan));
+    if (targets) {  // the job's population / fitness live elsewhere (a device GA's buffers)
+      ls->jobs.back().pop = (*targets)[j].first;
+      ls->jobs.back().fitness = (*targets)[j].second;
+    }
     for (int p = 0; p < jobs[j].second->P; ++p) indmap.push_back(make_int2((int)j, p));
   }
   std::vector<WorkItem> all;
@@ -1433,6 +1592,7 @@ int plan_build(Engine* e, int P, Plan** out) {
   plan->Pstride = (P + 31) & ~31;
   const int K = consts_per_individual(d);
   GPUGA_TRY(e->alloc(&plan->d_consts, (size_t)K * plan->Pstride));
+  if (const int K64 = consts64_per_individual(d)) GPUGA_TRY(e->alloc(&plan->d_consts64, (size_t)K64 * plan->Pstride));
   if (d.potential_type == 3) GPUGA_TRY(e->alloc(&plan->d_weights, (size_t)d.num_vars * plan->Pstride));
   GPUGA_TRY(e->alloc(&plan->d_res, (size_t)P * d.Nc * kResK));
   GPUGA_TRY(e->alloc(&plan->d_fitness, (size_t)P));

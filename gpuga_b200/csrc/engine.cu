@@ -14,6 +14,7 @@ Engine::~Engine() {
   plans.clear();  // graphs, pinned staging and launch sets
   for (void* ptr : allocations) cudaFree(ptr);
   if (p_out) cudaFree(p_out);
+  if (p_w) cudaFree(p_w);
   if (stream) cudaStreamDestroy(stream);
 }
 

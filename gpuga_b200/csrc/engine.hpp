@@ -7,9 +7,10 @@
 //   bonds    nbr[B], rev[B] (reverse bond), rev_sm[B] (the reverse bond's slot * Na + atom,
 //            local to the configuration), ptype[B] (pair set / RI pair type),
 //            g32[B] float4 (unit vector, d; not kept for RI), g64[B] double4 (x,y,z,d),
-//            gri[B] float4 (RI build scratch: FP64 remainder of d, 1/d^6 and the
-//            damped Coulomb energy / force pieces)
-//            RI: rg32 / rgri / rseg, each atom's evaluated pairs grouped by pair type
+//            d64[B] (Tersoff: the FP64 bond length again, for the FP64 pair terms)
+//            RI: rg32 / rdl / rseg, each atom's pairs of the pair types whose Buckingham or
+//            Morse term can be nonzero, grouped by pair type; ri_atom_lin / ri_cfg_lin, the
+//            FP64 geometric sums of the terms that are linear in the parameters
 //   targets  force_ref[3N], E_ref[Nc], W_ref[6Nc] (FP64 copies of the FP32 inputs)
 //
 // Bond vectors use the periodic image chosen by the reference's FP32 rule and
@@ -32,6 +33,8 @@ constexpr int kBlock = 256;           // threads per CTA of the batched kernels
 constexpr int kWarps = kBlock / 32;
 constexpr int kResK = 8;              // per (individual, config): E, W[6], sum|dF|^2
 constexpr int kMaxConsts = 32;        // per-individual FP32 constants of the batched kernels
+constexpr int kRiAtomLin = 27;        // RI linear force sums per force atom: 3 pair types x 3 x xyz
+constexpr int kRiCfgLin = 66;         // RI linear energy/virial sums per configuration: 3 x (4 + 3 x 6)
 
 struct DevSet {
   int Nc = 0, Nc_force = 0, N = 0, N_force = 0, B = 0, max_Na = 0, max_Z = 0;
@@ -50,21 +53,27 @@ struct DevSet {
   uint8_t* ptype = nullptr;
   float4* g32 = nullptr;
   double4* g64 = nullptr;
-  float4* gri = nullptr;   // RI build scratch (freed once rg32 / rgri exist)
-  // RI batched lists: per atom the pairs its work items evaluate (the full list for force
-  // configurations, the half list for energy/virial ones) grouped by pair type, in list order
-  // within a type: rseg[i] = (start, start of type 1, start of type 2, end) into rg32 / rgri
-  float4* rg32 = nullptr;
-  float4* rgri = nullptr;
+  double* d64 = nullptr;   // Tersoff: FP64 bond lengths (the FP64 pair terms)
+  float* tdl = nullptr;    // Tersoff: d - (float)d (the FP32 pair terms' correction)
+  // RI batched lists: per atom the pairs its work items evaluate pair by pair (the full list
+  // for force configurations, the half list for energy/virial ones; only pair types whose
+  // Buckingham or Morse term can be nonzero, ri_active) grouped by pair type, in list order
+  // within a type: rseg[i] = (start, start of type 1, start of type 2, end) into rg32 / rdl
+  float4* rg32 = nullptr;  // (unit vector, d)
+  float* rdl = nullptr;    // d - (float)d
   int4* rseg = nullptr;
+  int ri_active = 0;       // bit t: pair type t is evaluated pair by pair
+  // RI: the damped, shifted Coulomb and the dispersion terms are linear in the per-individual
+  // constants (qq_t, qq_t v_rc, qq_t dv_rc, C_t), so their geometric sums over all pairs are
+  // formed once in FP64: per force atom [kRiAtomLin], per energy/virial configuration
+  // [kRiCfgLin] (layouts at ri_linear_atoms, geometry.cu)
+  double* ri_atom_lin = nullptr;
+  double* ri_cfg_lin = nullptr;
   float* force_ref = nullptr;
   double* E_ref = nullptr;
   double* W_ref = nullptr;
   double norm_force = 0, norm_energy = 0, norm_virial = 0;
   float w_force = 0, w_energy = 0, w_stress = 0;
-  // RI: the Coulomb shift cutoff (parameter 10) is the same for every individual, so the
-  // shifted, damped Coulomb term is precomputed per bond in FP64 (gri.z, gri.w)
-  int ri_fixed_rc = 0;
   // RI: per configuration sum_i (q_i / q)^2 = cations + ratio^2 anions (the self-energy weight)
   double* ri_qsum = nullptr;
 };
@@ -91,9 +100,13 @@ struct DevView {
   const int* rev_sm;
   const uint8_t* ptype;
   const float4* g32;
+  const double* d64;
+  const float* tdl;
   const float4* rg32;
-  const float4* rgri;
+  const float* rdl;
   const int4* rseg;
+  const double* ri_atom_lin;
+  const double* ri_cfg_lin;
   const float* force_ref;
   const double* ri_qsum;
 };
@@ -107,12 +120,13 @@ struct NNTaper {
 // buffers of its evaluation.  Several jobs share the same launches.
 struct JobView {
   DevView v;
-  int potential_type, num_types, num_neurons, num_vars, P, Pstride, Nc_force, ri_fixed_rc, ri_self;
+  int potential_type, num_types, num_neurons, num_vars, P, Pstride, Nc_force, ri_self;
   NNTaper tp;
   const float* pop;      // [P][num_vars] in [0,1]
   const float* pmin;
   const float* pmax;
   float* consts;         // [K][Pstride]
+  double* consts64;      // RI: [K64][Pstride] FP64 constants of the linear terms
   float* weights;        // NN2B [num_vars][Pstride]
   double* res;           // [P][Nc][kResK]
   float* fdump;          // optional [P][3][N_force]
@@ -163,6 +177,7 @@ struct Plan {
   int P = 0;
   int Pstride = 0;
   float* d_consts = nullptr;   // [K][Pstride] per-individual constants
+  double* d_consts64 = nullptr; // RI: [K64][Pstride] FP64 constants of the linear terms
   float* d_weights = nullptr;  // NN2B weights [num_vars][Pstride]
   double* d_res = nullptr;     // [P][Nc][kResK]
   double* d_fitness = nullptr; // [P]
@@ -193,7 +208,7 @@ struct Engine {
   size_t device_bytes = 0;
   std::vector<void*> allocations;
   // plain-path scratch
-  double* s64 = nullptr;  // per-bond scratch (b, bp, fx, fy, fz) FP64
+  double* s64 = nullptr;  // per-bond scratch (S, A, f_ij x/y/z) FP64
   float* s32 = nullptr;
   double* p64_F = nullptr;
   double* p64_W = nullptr;
@@ -203,6 +218,8 @@ struct Engine {
   float* p32_pe = nullptr;
   double* p_out = nullptr;  // per-individual fitness + components of the plain path [4P]
   int p_out_cap = 0;
+  void* p_w = nullptr;      // plain-path NN2B weights of the evaluated parameter vectors
+  size_t p_w_bytes = 0;
   ~Engine();
   int dalloc(void** p, size_t bytes);
   template <class T>
@@ -225,7 +242,7 @@ int ref_layout_geometry(int Nc, int N, const int* Na, const int* Na_sum, const f
 struct RefPotentialScratch {
   double4* g64;  // [max_Na * N]
   int* rev;      // [max_Na * N]
-  float* f5;     // [5 * max_Na * N]: b, b', f_ij x/y/z
+  float* f5;     // [5 * max_Na * N]: per-bond S, A, f_ij x/y/z
   float* w;      // NN2B weights [num_vars]
 };
 size_t ref_potential_scratch_bytes(int potential_type, int num_neurons, int N, int max_Na);
@@ -237,9 +254,12 @@ int ref_potential_find_force(int potential_type, int num_neurons, const float* p
 // batched.cu
 int plan_build(Engine* e, int P, Plan** out);
 int consts_per_individual(const DevSet& d);
+int consts64_per_individual(const DevSet& d);
 JobView make_job_view(const Engine* e, const Plan* plan);
-// Builds the shared launches of the given jobs (one engine + plan each).
-int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSet* ls);
+// Builds the shared launches of the given jobs (one engine + plan each); `targets`, when given,
+// names each job's population and fitness buffers (default: the plan's own).
+int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSet* ls,
+                    const std::vector<std::pair<const float*, double*>>* targets = nullptr);
 // Enqueues one generation of every job of the set on `st` (force launches on a side stream).
 int launchset_enqueue(LaunchSet* ls, cudaStream_t st);
 int launchset_collect_timing(LaunchSet* ls);
@@ -277,7 +297,8 @@ int ga_batch_build(const std::vector<DeviceGA*>& jobs, LaunchSet* ls, GABatch** 
 void ga_batch_free(GABatch* b);
 int ga_batch_window(GABatch* B, int b, int n, bool use_graph, bool timed, cudaStream_t st);
 int ga_batch_wait(GABatch* B, int b);
-int ga_batch_generation_ms(GABatch* B, int n, std::vector<double>* ms);
+// device time of each generation of the last timed window on plan buffer b
+int ga_batch_generation_ms(GABatch* B, int b, int n, std::vector<double>* ms);
 
 // engine.cu
 int engine_create(const PotentialSpec& spec, TrainingSet&& ts, const gpuga_options& opt, Engine** out);

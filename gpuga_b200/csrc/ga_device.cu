@@ -145,14 +145,14 @@ struct GABatch {
   size_t rank_smem = 0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   cudaEvent_t done[2] = {nullptr, nullptr};
-  std::vector<cudaEvent_t> gen_ev;  // per-generation timing events of the last window
+  std::vector<cudaEvent_t> gen_ev[2];  // per-generation timing events of the last window on buffer b
   ~GABatch() {
     for (int b = 0; b < 2; ++b) {
       if (graph[b]) cudaGraphExecDestroy(graph[b]);
       if (done[b]) cudaEventDestroy(done[b]);
       cudaFree(d_table[b]);
+      for (cudaEvent_t e : gen_ev[b]) cudaEventDestroy(e);
     }
-    for (cudaEvent_t e : gen_ev) cudaEventDestroy(e);
     cudaFree(d_rank_map);
     cudaFree(d_breed_map);
     cudaFree(d_mut_map);
@@ -391,19 +391,20 @@ int ga_batch_window(GABatch* B, int b, int n, bool use_graph, bool timed, cudaSt
     cudaGraphDestroy(g);
     GPUGA_CUDA(ie);
   }
-  while (timed && (int)B->gen_ev.size() < n + 1) {
+  std::vector<cudaEvent_t>& ev = B->gen_ev[b];
+  while (timed && (int)ev.size() < n + 1) {
     cudaEvent_t e;
     GPUGA_CUDA(cudaEventCreate(&e));
-    B->gen_ev.push_back(e);
+    ev.push_back(e);
   }
-  if (timed) GPUGA_CUDA(cudaEventRecord(B->gen_ev[0], st));
+  if (timed) GPUGA_CUDA(cudaEventRecord(ev[0], st));
   for (int k = 0; k < n; ++k) {
     if (use_graph) {
       GPUGA_CUDA(cudaGraphLaunch(B->graph[b], st));
     } else {
       GPUGA_TRY(enqueue_generation(B, b, st));
     }
-    if (timed) GPUGA_CUDA(cudaEventRecord(B->gen_ev[k + 1], st));
+    if (timed) GPUGA_CUDA(cudaEventRecord(ev[k + 1], st));
   }
   for (DeviceGA* s : B->jobs)
     GPUGA_CUDA(cudaMemcpyAsync(s->h_hist[b], s->d_hist[b], sizeof(float) * (size_t)n * (s->d + 1),
@@ -417,10 +418,10 @@ int ga_batch_wait(GABatch* B, int b) {
   return GPUGA_OK;
 }
 
-int ga_batch_generation_ms(GABatch* B, int n, std::vector<double>* ms) {
+int ga_batch_generation_ms(GABatch* B, int b, int n, std::vector<double>* ms) {
   for (int k = 0; k < n; ++k) {
     float t = 0.f;
-    GPUGA_CUDA(cudaEventElapsedTime(&t, B->gen_ev[k], B->gen_ev[k + 1]));
+    GPUGA_CUDA(cudaEventElapsedTime(&t, B->gen_ev[b][k], B->gen_ev[b][k + 1]));
     ms->push_back(t);
   }
   return GPUGA_OK;

@@ -198,12 +198,14 @@ constexpr double kRiAlpha = 0.2;                  // ri.cu:26
 constexpr double kRiPiFactor = 0.225675833419103;  // ri.cu:28, 2*alpha/sqrt(pi)
 
 // Per atom: FP64 bond vectors for the FP32-chosen image, FP32 unit vectors,
-// reverse bonds, half-list start and pair types.
+// reverse bonds, half-list start and pair types; where asked for (dl, d64 not null)
+// also the FP64 remainder d - (float)d of each bond length and the FP64 length itself.
 __global__ void bond_geometry(int N, const int* __restrict__ atom_cfg, const float* __restrict__ box,
                               const float* __restrict__ r, const int* __restrict__ type, const int* __restrict__ off,
                               const int* __restrict__ nbr, const float* __restrict__ img, int potential_type,
-                              int num_types, double rc_fixed, double4* __restrict__ g64, float4* __restrict__ g32,
-                              float4* __restrict__ gri, int* __restrict__ rev, int* __restrict__ half_off,
+                              int num_types, double4* __restrict__ g64, float4* __restrict__ g32,
+                              float* __restrict__ dl, double* __restrict__ d64, int* __restrict__ rev,
+                              int* __restrict__ half_off,
                               uint8_t* __restrict__ ptype) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
@@ -220,23 +222,9 @@ __global__ void bond_geometry(int N, const int* __restrict__ atom_cfg, const flo
     const double d = sqrt(dx * dx + dy * dy + dz * dz);
     g64[b] = make_double4(dx, dy, dz, d);
     g32[b] = make_float4((float)(dx / d), (float)(dy / d), (float)(dz / d), (float)d);
-    if (gri) {
-      const double dinv = 1.0 / d;
-      const double dinv3 = dinv * dinv * dinv;
-      const double e1 = erfc(kRiAlpha * d) * dinv;
-      const double e2 = e1 * dinv + kRiPiFactor * dinv * exp(-kRiAlpha * kRiAlpha * d * d);
-      if (rc_fixed > 0) {
-        // whole shifted-force Coulomb term (ri.cu:92-94) for the common cutoff, in FP64
-        const double v_rc = erfc(kRiAlpha * rc_fixed) / rc_fixed;
-        const double dv_rc = -erfc(kRiAlpha * rc_fixed) / (rc_fixed * rc_fixed) -
-                             kRiPiFactor * exp(-kRiAlpha * kRiAlpha * rc_fixed * rc_fixed) / rc_fixed;
-        gri[b] = make_float4((float)(d - (double)(float)d), (float)(dinv3 * dinv3),
-                             (float)(e1 - v_rc - dv_rc * (d - rc_fixed)), (float)(e2 + dv_rc));
-      } else {
-        gri[b] = make_float4((float)(d - (double)(float)d), (float)(dinv3 * dinv3), (float)e1, (float)e2);
-      }
-    }
-    int rb = off[j];  // minimal_tersoff.cu:368: slot 0 when the reverse is absent
+    if (dl) dl[b] = (float)(d - (double)(float)d);
+    if (d64) d64[b] = d;
+  int rb = off[j];  // minimal_tersoff.cu:368: slot 0 when the reverse is absent
     for (int k = off[j]; k < off[j + 1]; ++k)
       if (nbr[k] == i) {
         rb = k;
@@ -266,12 +254,13 @@ __global__ void reverse_slots(int N, const int* __restrict__ atom_cfg, const int
   }
 }
 
-// RI: each atom's evaluated pairs (full list for force configurations, i < N_force;
-// half list otherwise) copied grouped by pair type, list order kept within a type.
-__global__ void ri_group(int N, int N_force, const int* __restrict__ off, const int* __restrict__ half_off,
+// RI: each atom's pairs that are evaluated pair by pair (full list for force
+// configurations, i < N_force; half list otherwise; pair types in the `active` mask
+// only) copied grouped by pair type, list order kept within a type.
+__global__ void ri_group(int N, int N_force, int active, const int* __restrict__ off, const int* __restrict__ half_off,
                          const uint8_t* __restrict__ ptype, const float4* __restrict__ g32,
-                         const float4* __restrict__ gri, const int* __restrict__ start, float4* __restrict__ rg32,
-                         float4* __restrict__ rgri, int4* __restrict__ rseg) {
+                         const float* __restrict__ dl, const int* __restrict__ start, float4* __restrict__ rg32,
+                         float* __restrict__ rdl, int4* __restrict__ rseg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const int bb = i < N_force ? off[i] : half_off[i], be = off[i + 1];
@@ -279,14 +268,78 @@ __global__ void ri_group(int N, int N_force, const int* __restrict__ off, const 
   int seg[3];
   for (int t = 0; t < 3; ++t) {
     seg[t] = o;
+    if (!((active >> t) & 1)) continue;
     for (int b = bb; b < be; ++b) {
       if (ptype[b] != t) continue;
       rg32[o] = g32[b];
-      rgri[o] = gri[b];
+      rdl[o] = dl[b];
       ++o;
     }
   }
   rseg[i] = make_int4(seg[0], seg[1], seg[2], o);
+}
+
+// RI terms that are linear in the per-individual constants (ri.cu:77-110): for pair type t
+//   U_lin(d) = qq_t [ec(d) - v_rc - dv_rc (d - rc)] - C_t / d^6,
+//   dU_lin/dd = -qq_t [gc(d) + dv_rc] + 6 C_t / d^7,
+//   ec = erfc(alpha d) / d,  gc = erfc(alpha d) / d^2 + (2 alpha / sqrt(pi)) e^{-alpha^2 d^2} / d.
+// Their geometric sums, in FP64, one thread per atom:
+//   force atom i (full list), out_atom[i][t*9 + 3m + a]: m = 0 sum gc u_a, 1 sum u_a, 2 sum u_a / d^7
+//     (F_i = sum_j dU/dd u_ij);
+//   energy/virial atom i (half list, j > i), out_ev[i][t*22 + ...]: [0..3] sum ec, count, sum d,
+//     sum 1/d^6; [4 + 6m + k] with m = 0 sum d gc uu, 1 sum d uu, 2 sum uu / d^6, k = xx, yy, zz,
+//     xy, yz, zx (W = -sum_pairs d dU/dd u (x) u).
+__global__ void ri_linear_atoms(int N, int N_force, const int* __restrict__ off, const int* __restrict__ half_off,
+                                const uint8_t* __restrict__ ptype, const double4* __restrict__ g64,
+                                double* __restrict__ out_atom, double* __restrict__ out_ev) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const bool force = i < N_force;
+  double acc[kRiCfgLin];
+  for (int k = 0; k < kRiCfgLin; ++k) acc[k] = 0.0;
+  for (int b = force ? off[i] : half_off[i]; b < off[i + 1]; ++b) {
+    const double4 q = g64[b];
+    const double d = q.w, id = 1.0 / d, id2 = id * id, id6 = id2 * id2 * id2;
+    const double u[3] = {q.x * id, q.y * id, q.z * id};
+    const double ec = erfc(kRiAlpha * d) * id;
+    const double gc = ec * id + kRiPiFactor * exp(-kRiAlpha * kRiAlpha * d * d) * id;
+    const int t = ptype[b];
+    if (force) {
+      double* a = acc + 9 * t;
+      for (int c = 0; c < 3; ++c) {
+        a[c] += gc * u[c];
+        a[3 + c] += u[c];
+        a[6 + c] += id6 * id * u[c];
+      }
+    } else {
+      double* a = acc + 22 * t;
+      a[0] += ec;
+      a[1] += 1.0;
+      a[2] += d;
+      a[3] += id6;
+      const double uu[6] = {u[0] * u[0], u[1] * u[1], u[2] * u[2], u[0] * u[1], u[1] * u[2], u[2] * u[0]};
+      for (int k = 0; k < 6; ++k) {
+        a[4 + k] += d * gc * uu[k];
+        a[10 + k] += d * uu[k];
+        a[16 + k] += id6 * uu[k];
+      }
+    }
+  }
+  if (force) {
+    for (int k = 0; k < kRiAtomLin; ++k) out_atom[(size_t)i * kRiAtomLin + k] = acc[k];
+  } else {
+    for (int k = 0; k < kRiCfgLin; ++k) out_ev[(size_t)i * kRiCfgLin + k] = acc[k];
+  }
+}
+
+// Per energy/virial configuration c >= Nc_force: the atoms' sums in atom order (thread k = sum k).
+__global__ void ri_linear_configs(int Nc, int Nc_force, const int* __restrict__ Na, const int* __restrict__ Na_sum,
+                                  const double* __restrict__ ev, double* __restrict__ out_cfg) {
+  const int c = Nc_force + blockIdx.x, k = threadIdx.x;
+  if (c >= Nc || k >= kRiCfgLin) return;
+  double s = 0.0;
+  for (int i = Na_sum[c]; i < Na_sum[c] + Na[c]; ++i) s += ev[(size_t)i * kRiCfgLin + k];
+  out_cfg[(size_t)c * kRiCfgLin + k] = s;
 }
 
 // Bond geometry for lists in the reference layout NL[k*N + i]: the FP32 rule
@@ -423,6 +476,21 @@ void build_cell_lists(const Engine* e, CellLists* cl) {
   }
 }
 
+// Pair types whose Buckingham or Morse term can be nonzero for some individual: type t is left
+// out of the pair-by-pair lists when its bounds fix A_t = 0 with rho_t > 0 (A e^{-d/rho} is then
+// exactly zero) and, for the cation-anion type, the Morse D0 is fixed at 0 as well.
+static int ri_active_types(const PotentialSpec& sp) {
+  if (sp.pmin.size() < 15 || sp.pmax.size() < 15) return 7;
+  int mask = 0;
+  for (int t = 0; t < 3; ++t) {
+    const int a = 1 + 3 * t, rho = 2 + 3 * t;
+    const bool zero_buck = sp.pmin[a] == 0.0f && sp.pmax[a] == 0.0f && sp.pmin[rho] > 0.0f;
+    const bool zero_morse = t != 1 || (sp.pmin[11] == 0.0f && sp.pmax[11] == 0.0f);
+    if (!(zero_buck && zero_morse)) mask |= 1 << t;
+  }
+  return mask;
+}
+
 int build_geometry(Engine* e) {
   DevSet& d = e->d;
   const TrainingSet& ts = e->ts;
@@ -516,51 +584,71 @@ int build_geometry(Engine* e) {
   GPUGA_CUDA(cudaMemcpyAsync(d_atom_cfg, atom_cfg.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
 
   GPUGA_TRY(e->alloc(&d.g64, std::max(B, 1)));
-  // RI evaluates its type-grouped copies (rg32 / rgri, below): there g32 and gri are scratch
+  // RI evaluates its type-grouped copies (rg32 / rdl, below): there g32 and dl are scratch
   const bool ri = is_ri_type(d.potential_type);
+  float* dl = nullptr;
   if (ri) {
     GPUGA_CUDA(cudaMalloc(&d.g32, sizeof(float4) * std::max(B, 1)));
-    GPUGA_CUDA(cudaMalloc(&d.gri, sizeof(float4) * std::max(B, 1)));
+    GPUGA_CUDA(cudaMalloc(&dl, sizeof(float) * std::max(B, 1)));
   } else {
     GPUGA_TRY(e->alloc(&d.g32, std::max(B, 1)));
   }
   GPUGA_TRY(e->alloc(&d.rev, std::max(B, 1)));
   GPUGA_TRY(e->alloc(&d.half_off, N));
   GPUGA_TRY(e->alloc(&d.ptype, std::max(B, 1)));
-  double rc_fixed = 0.0;
-  if (ri && e->spec.pmin.size() > 10 && e->spec.pmin[10] == e->spec.pmax[10] &&
-      e->spec.pmin[10] > 0) {
-    rc_fixed = e->spec.pmin[10];
-    d.ri_fixed_rc = 1;
+  const bool tersoff = d.potential_type == 1 || d.potential_type == 2;
+  if (tersoff) {
+    GPUGA_TRY(e->alloc(&d.d64, std::max(B, 1)));
+    GPUGA_TRY(e->alloc(&d.tdl, std::max(B, 1)));
   }
   bond_geometry<<<(N + 127) / 128, 128, 0, st>>>(N, d_atom_cfg, d.h, d.r, d.type, d.off, d.nbr, img,
-                                                 ri ? 0 : d.potential_type, d.num_types, rc_fixed, d.g64, d.g32, d.gri, d.rev,
-                                                 d.half_off, d.ptype);
+                                                 ri ? 0 : d.potential_type, d.num_types, d.g64, d.g32,
+                                                 ri ? dl : d.tdl, d.d64, d.rev, d.half_off, d.ptype);
   GPUGA_CUDA(cudaGetLastError());
   GPUGA_TRY(e->alloc(&d.rev_sm, std::max(B, 1)));
   reverse_slots<<<(N + 127) / 128, 128, 0, st>>>(N, d_atom_cfg, d.Na, d.Na_sum, d.off, d.nbr, d.rev, d.rev_sm);
   GPUGA_CUDA(cudaGetLastError());
   if (ri) {
+    d.ri_active = ri_active_types(e->spec);
     std::vector<int> half(N), start(N + 1, 0);
+    std::vector<uint8_t> pt(std::max(B, 1));
     GPUGA_CUDA(cudaMemcpyAsync(half.data(), d.half_off, sizeof(int) * N, cudaMemcpyDeviceToHost, st));
+    GPUGA_CUDA(cudaMemcpyAsync(pt.data(), d.ptype, (size_t)B, cudaMemcpyDeviceToHost, st));
     GPUGA_CUDA(cudaStreamSynchronize(st));
-    for (int i = 0; i < N; ++i)
-      start[i + 1] = start[i] + e->h_off[i + 1] - (i < ts.N_force ? e->h_off[i] : half[i]);
+    // the host has the lists already (h_off); nbr comes back below, ptype just now
+    for (int i = 0; i < N; ++i) {
+      int n = 0;
+      for (int b = i < ts.N_force ? e->h_off[i] : half[i]; b < e->h_off[i + 1]; ++b) n += (d.ri_active >> pt[b]) & 1;
+      start[i + 1] = start[i] + n;
+    }
     int* d_start = nullptr;
     GPUGA_CUDA(cudaMalloc(&d_start, sizeof(int) * (N + 1)));
     GPUGA_CUDA(cudaMemcpyAsync(d_start, start.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice, st));
     GPUGA_TRY(e->alloc(&d.rg32, std::max(start[N], 1)));
-    GPUGA_TRY(e->alloc(&d.rgri, std::max(start[N], 1)));
+    GPUGA_TRY(e->alloc(&d.rdl, std::max(start[N], 1)));
     GPUGA_TRY(e->alloc(&d.rseg, N));
-    ri_group<<<(N + 127) / 128, 128, 0, st>>>(N, ts.N_force, d.off, d.half_off, d.ptype, d.g32, d.gri, d_start, d.rg32,
-                                              d.rgri, d.rseg);
+    ri_group<<<(N + 127) / 128, 128, 0, st>>>(N, ts.N_force, d.ri_active, d.off, d.half_off, d.ptype, d.g32, dl,
+                                              d_start, d.rg32, d.rdl, d.rseg);
     GPUGA_CUDA(cudaGetLastError());
+    // FP64 sums of the linear terms
+    double* ev = nullptr;
+    GPUGA_CUDA(cudaMalloc(&ev, sizeof(double) * kRiCfgLin * (size_t)std::max(N, 1)));
+    GPUGA_TRY(e->alloc(&d.ri_atom_lin, (size_t)kRiAtomLin * std::max(ts.N_force, 1)));
+    GPUGA_TRY(e->alloc(&d.ri_cfg_lin, (size_t)kRiCfgLin * Nc));
+    GPUGA_CUDA(cudaMemsetAsync(d.ri_cfg_lin, 0, sizeof(double) * kRiCfgLin * (size_t)Nc, st));
+    ri_linear_atoms<<<(N + 127) / 128, 128, 0, st>>>(N, ts.N_force, d.off, d.half_off, d.ptype, d.g64, d.ri_atom_lin,
+                                                     ev);
+    GPUGA_CUDA(cudaGetLastError());
+    if (Nc > ts.Nc_force) {
+      ri_linear_configs<<<Nc - ts.Nc_force, 96, 0, st>>>(Nc, ts.Nc_force, d.Na, d.Na_sum, ev, d.ri_cfg_lin);
+      GPUGA_CUDA(cudaGetLastError());
+    }
     GPUGA_CUDA(cudaStreamSynchronize(st));
+    cudaFree(ev);
     cudaFree(d_start);
     cudaFree(d.g32);
-    cudaFree(d.gri);
+    cudaFree(dl);
     d.g32 = nullptr;
-    d.gri = nullptr;
   }
 
   GPUGA_CUDA(cudaStreamSynchronize(st));

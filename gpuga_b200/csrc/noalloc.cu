@@ -13,9 +13,13 @@
 //
 // The first call on a device resolves the array's device address
 // (cudaGetSymbolAddress, with that device current); make that first call
-// before any stream capture.  Every call on a device uses the same array, so
+// before any stream capture.  The address is kept until the process exits: a
+// cudaDeviceReset unloads the module, so the entry point must not be used on
+// that device afterwards.  Every call on a device uses the same array, so
 // calls whose work overlaps on the GPU (two streams, two threads) race on it;
 // serialise them.  Each call zeroes the part of the array it uses before use.
+// `params` is a host array (read during the call; the NN2B weights are copied
+// from it into the scratch), every other array a device array.
 #include <mutex>
 
 #include "engine.hpp"

@@ -1,60 +1,141 @@
-// Plain path: one individual per launch sequence, one thread per atom, the
-// reference's three-step Tersoff structure (minimal_tersoff.cu:122-405) and
-// owner-computes pair loops (ri.cu:112-189, nn2b.cu:94-173), templated on the
-// arithmetic type.  FP64 is the denominator of the batched engine's speed-up
-// and the device-side FP64 reference; FP32 gives the reference's float outputs.
+// Plain path: one parameter vector per launch sequence, one thread per atom,
+// every arithmetic step in the template type T.  T = double is the FP64
+// reference on the device (gpuga_find_force64, gpuga_predict) and the
+// denominator of the batched engine's speed-up ("plain FP64, one individual per
+// launch"); T = float serves the reference's FP32 Potential entry points.
+//
+// The formulation is the batched engine's (batched.cu): unit bond vectors,
+// the bond-order derivative folded into per-bond scalars and each partial
+// force f_ij assembled from a radial and a perpendicular part.  The per-bond
+// scalars live in global scratch instead of registers, so an atom may have any
+// number of neighbors.  Output layouts are the reference's (potential.cuh:28-40):
+// F[3][N], W[6][N] (xx, yy, zz, xy, yz, zx) and pe[N] per atom.
 #include <cmath>
 
 #include "engine.hpp"
 
 namespace gpuga {
 
+// -------------------------------------------------------------------- math by argument type
+__device__ __forceinline__ float m_exp(float x) { return expf(x); }
+__device__ __forceinline__ double m_exp(double x) { return exp(x); }
+__device__ __forceinline__ float m_log(float x) { return logf(x); }
+__device__ __forceinline__ double m_log(double x) { return log(x); }
+__device__ __forceinline__ float m_log1p(float x) { return log1pf(x); }
+__device__ __forceinline__ double m_log1p(double x) { return log1p(x); }
+__device__ __forceinline__ float m_erfc(float x) { return erfcf(x); }
+__device__ __forceinline__ double m_erfc(double x) { return erfc(x); }
+__device__ __forceinline__ float m_tanh(float x) { return tanhf(x); }
+__device__ __forceinline__ double m_tanh(double x) { return tanh(x); }
+__device__ __forceinline__ void m_sincos(float x, float* s, float* c) { sincosf(x, s, c); }
+__device__ __forceinline__ void m_sincos(double x, double* s, double* c) { sincos(x, s, c); }
+
+// Cosine taper between r1 and r2 (minimal_tersoff.cu:77-90; nn2b.cu:80-92 with its own r1, r2):
+// 1 below r1, 0 from r2 on, (1 + cos(pf (d - r1))) / 2 between; dfc = d fc / d d.
 template <class T>
-struct PT {  // minimal Tersoff constants
-  T D0[2], A[2], R0[2], S[2], EN, BETA, H, R1, R2, PF, MHON;
-};
+__device__ __forceinline__ void taper(T r1, T r2, T pf, T d, T& fc, T& dfc) {
+  fc = T(0);
+  dfc = T(0);
+  if (d < r1) {
+    fc = T(1);
+  } else if (d < r2) {
+    T s, c;
+    m_sincos(pf * (d - r1), &s, &c);
+    fc = T(0.5) * (T(1) + c);
+    dfc = T(-0.5) * pf * s;
+  }
+}
+
+// ------------------------------------------------------------------------ parameter sets
+// Minimal Tersoff (minimal_tersoff.cu:39-75) as the engine derives it: per pair set s (0 for
+// equal types, 1 otherwise) fr = cr e^{-lr (d - r0)}, fa = ca e^{-la (d - r0)} with
+// lr = sqrt(2S) A, la = sqrt(2/S) A, cr = D0/(S-1), ca = S D0/(S-1); then the bond order
+// b = (1 + zeta^n)^mhon, mhon = -1/(2n), zeta = sum fc beta (cos - h)^2.
 template <class T>
-struct PR {  // RI constants (ri.cu:21-25); self: K_C S(rc) of the optional self energy (0 when off)
-  T a[3], b[3], c[3], qq[3], v_rc, dv_rc, cutoff, d0, alpha, r0, s, self;
+struct TersoffSet {
+  T cr[2], ca[2], lr[2], la[2], r0[2];
+  T n, beta, h, r1, r2, pf, mhon;
 };
+
+template <class T>
+TersoffSet<T> tersoff_set(const double* p, int num_types) {
+  TersoffSet<T> t;
+  const int off = num_types == 2 ? 4 : 0;
+  for (int s = 0; s < 2; ++s) {
+    const double* q = p + ((num_types == 2 && s == 1) ? 4 : 0);  // D0, A, r0, S of the set
+    const double D0 = q[0], A = q[1], R0 = q[2], S = q[3];
+    t.cr[s] = (T)(D0 / (S - 1.0));
+    t.ca[s] = (T)(S * D0 / (S - 1.0));
+    t.lr[s] = (T)(sqrt(2.0 * S) * A);
+    t.la[s] = (T)(sqrt(2.0 / S) * A);
+    t.r0[s] = (T)R0;
+  }
+  const double n = p[4 + off], r1 = p[7 + off], r2 = p[8 + off];
+  t.n = (T)n;
+  t.beta = (T)p[5 + off];
+  t.h = (T)p[6 + off];
+  t.r1 = (T)r1;
+  t.r2 = (T)r2;
+  t.pf = (T)(M_PI / (r2 - r1));
+  t.mhon = (T)(-0.5 / n);
+  return t;
+}
+
+// Rigid ion (ri.cu:21-110): per pair type t = type_i + type_j Buckingham A, 1/rho, C and the
+// charge product qq (K_C included), the shifted damped Coulomb term with cutoff rc, and the
+// cation-anion Morse pair with the Tersoff-style constants above; self = K_C S(rc) of the optional
+// self energy (0 when off).
+template <class T>
+struct RigidIon {
+  T A[3], inv_rho[3], C[3], qq[3];
+  T rc, v_rc, dv_rc, cr, ca, lr, la, r0, self;
+};
+
+constexpr double kCoulomb = 14.399645;      // ri.cu:29
+constexpr double kAlpha = 0.2;              // ri.cu:26
+constexpr double kTwoOverSqrtPi = 1.1283791670955126;
 
 // Damped-Coulomb self energy per K_C q_i^2 (develop/hfo2/find_E.m:10-13).
 inline double ri_self_factor(double rc) {
-  const double alpha = 0.2, pif = 0.225675833419103;
-  return alpha / sqrt(M_PI) + erfc(alpha * rc) / rc + 0.5 * pif * exp(-alpha * alpha * rc * rc);
+  return kAlpha / sqrt(M_PI) + erfc(kAlpha * rc) / rc + 0.5 * (kTwoOverSqrtPi * kAlpha) * exp(-kAlpha * kAlpha * rc * rc);
 }
-struct PN {
-  int n;
+
+template <class T>
+RigidIon<T> rigid_ion_set(const double* p, int potential_type, bool with_self) {
+  RigidIon<T> r;
+  const double q2 = p[0] * p[0] * kCoulomb, ratio = ri_charge_ratio(potential_type);
+  r.qq[0] = (T)q2;
+  r.qq[1] = (T)(ratio * q2);
+  r.qq[2] = (T)(ratio * ratio * q2);
+  for (int t = 0; t < 3; ++t) {
+    r.A[t] = (T)p[1 + 3 * t];
+    r.inv_rho[t] = (T)(1.0 / p[2 + 3 * t]);
+    r.C[t] = (T)p[3 + 3 * t];
+  }
+  const double rc = p[10], D0 = p[11], al = p[12], S = p[14];
+  const double erfc_rc = erfc(kAlpha * rc);
+  r.rc = (T)rc;
+  r.v_rc = (T)(erfc_rc / rc);
+  r.dv_rc = (T)(-erfc_rc / (rc * rc) - kTwoOverSqrtPi * kAlpha * exp(-kAlpha * kAlpha * rc * rc) / rc);
+  r.cr = (T)(D0 / (S - 1.0));
+  r.ca = (T)(S * D0 / (S - 1.0));
+  r.lr = (T)(sqrt(2.0 * S) * al);
+  r.la = (T)(sqrt(2.0 / S) * al);
+  r.r0 = (T)p[13];
+  r.self = with_self ? (T)ri_self_factor(rc) : T(0);
+  return r;
+}
+
+// NN 2-body taper (nn2b.cuh:36-38 by default) and the force order of nn2b.cu:147-148.
+struct MlpTaper {
   double r1, r2, pf;
   int consistent;
 };
 
-template <class T>
-__device__ __forceinline__ T texp(T x) {
-  return exp(x);
-}
-template <>
-__device__ __forceinline__ float texp<float>(float x) {
-  return expf(x);
-}
-
-template <class T>
-__device__ __forceinline__ void fcut(T r1, T r2, T pf, T d, T& fc, T& fcp) {
-  if (d < r1) {
-    fc = 1;
-    fcp = 0;
-  } else if (d < r2) {
-    fc = T(0.5) * cos(pf * (d - r1)) + T(0.5);
-    fcp = -sin(pf * (d - r1)) * pf * T(0.5);
-  } else {
-    fc = 0;
-    fcp = 0;
-  }
-}
-
-// Neighbor-list layouts: the engine's CSR lists, or the reference's
-// NL[k*N + i] (neighbor.cu:61) for the drop-in Potential entry points.  A bond
-// slot indexes the per-bond arrays (geometry, reverse slot, scratch).
+// --------------------------------------------------------------------------- list layouts
+// The engine's CSR lists, or the reference's NL[k*N + i] (neighbor.cu:61) for the
+// drop-in Potential entry points.  A bond's slot indexes the per-bond arrays
+// (geometry, reverse slot, scratch).
 struct CsrLayout {
   const int* off;
   const int* nbr;
@@ -71,245 +152,211 @@ struct RefLayout {
   __device__ __forceinline__ int nb(int i, int k) const { return NL[(size_t)k * N + i]; }
 };
 
+// Bond geometry (x, y, z, d) in FP64 as unit vector and length in T.
 template <class T>
-__device__ __forceinline__ void bond(const double4* g, int b, T& x, T& y, T& z, T& d) {
-  const double4 q = g[b];
-  x = (T)q.x;
-  y = (T)q.y;
-  z = (T)q.z;
-  d = (T)q.w;
-}
+struct Bond {
+  T ux, uy, uz, d;
+  __device__ __forceinline__ explicit Bond(const double4& q) {
+    const double inv = 1.0 / q.w;
+    ux = (T)(q.x * inv);
+    uy = (T)(q.y * inv);
+    uz = (T)(q.z * inv);
+    d = (T)q.w;
+  }
+  __device__ __forceinline__ T dot(const Bond& o) const { return ux * o.ux + uy * o.uy + uz * o.uz; }
+};
 
-// step 1 (minimal_tersoff.cu:122-188): bond orders
+// ------------------------------------------------------------------------------- Tersoff
+// Per atom i, two passes over its bonds.
+//   1. bond order of every bond j: zeta_j = sum_{k != j} fc_k beta (cos_jk - h)^2,
+//      b_j = (1 + zeta_j^n)^mhon, db_j = d b / d zeta; the site energy
+//      pe_i = 1/2 sum_j fc_j (fr_j - b_j fa_j); per bond the scalars S_j = db_j fa_j and
+//      A_j = dfc_j (fr_j - b_j fa_j) + fc_j (fr'_j - b_j fa'_j) go to scratch.
+//   2. f_ij = dE_i / dr_ij = 1/2 [(A_j - dfc_j sum_k T_k g_jk - m_j sum_k q_jk cos_jk) u_j
+//                                 + m_j sum_k q_jk u_k]
+//      with T_k = S_k fc_k, g = beta (cos - h)^2, q_jk = beta (cos_jk - h)(S_j fc_k + T_k),
+//      m_j = -2 fc_j / d_j (the derivative of cos_jk along r_ij is (u_k - cos_jk u_j) / d_j).
 template <class T, class Lay>
-__global__ void p_tersoff1(int N, Lay L, const double4* __restrict__ g, PT<T> P, T* __restrict__ b,
-                           T* __restrict__ bp) {
+__global__ void plain_tersoff_bonds(int N, int num_types, const int* __restrict__ type, Lay L,
+                                    const double4* __restrict__ g, TersoffSet<T> P, T* __restrict__ sS,
+                                    T* __restrict__ sA, T* __restrict__ fx, T* __restrict__ fy, T* __restrict__ fz,
+                                    T* __restrict__ pe) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
+  const int Z = L.count(i), ti = type[i];
+  T site = T(0);
+  for (int j = 0; j < Z; ++j) {
+    const int sj = L.slot(i, j);
+    const Bond<T> bj(g[sj]);
+    T zeta = T(0);
+    for (int k = 0; k < Z; ++k) {
+      if (k == j) continue;
+      const Bond<T> bk(g[L.slot(i, k)]);
+      T fck, dfck;
+      taper(P.r1, P.r2, P.pf, bk.d, fck, dfck);
+      const T x = bj.dot(bk) - P.h;
+      zeta += fck * P.beta * x * x;
+    }
+    T b = T(1), db = T(0);
+    if (!(zeta < T(1.0e-16))) {  // minimal_tersoff.cu:178-185: b = 1, b' = 0 below 1e-16
+      const T zn = m_exp(P.n * m_log(zeta));
+      b = m_exp(P.mhon * m_log1p(zn));
+      db = T(-0.5) * b * zn / ((T(1) + zn) * zeta);
+    }
+    const int s = (num_types == 2 && ti != type[L.nb(i, j)]) ? 1 : 0;
+    const T t = bj.d - P.r0[s];
+    const T fr = P.cr[s] * m_exp(-P.lr[s] * t), fa = P.ca[s] * m_exp(-P.la[s] * t);
+    T fcj, dfcj;
+    taper(P.r1, P.r2, P.pf, bj.d, fcj, dfcj);
+    const T e = fr - b * fa;
+    site += T(0.5) * fcj * e;
+    sS[sj] = db * fa;
+    sA[sj] = dfcj * e + fcj * (-P.lr[s] * fr + b * P.la[s] * fa);
+  }
+  pe[i] = site;
+  for (int j = 0; j < Z; ++j) {
+    const int sj = L.slot(i, j);
+    const Bond<T> bj(g[sj]);
+    T fcj, dfcj;
+    taper(P.r1, P.r2, P.pf, bj.d, fcj, dfcj);
+    const T Sj = sS[sj];
+    T sum_tg = T(0), sum_qc = T(0), vx = T(0), vy = T(0), vz = T(0);
+    for (int k = 0; k < Z; ++k) {
+      if (k == j) continue;
+      const int sk = L.slot(i, k);
+      const Bond<T> bk(g[sk]);
+      T fck, dfck;
+      taper(P.r1, P.r2, P.pf, bk.d, fck, dfck);
+      const T Tk = sS[sk] * fck;
+      const T c = bj.dot(bk);
+      const T bx = P.beta * (c - P.h);
+      const T q = bx * (Sj * fck + Tk);
+      sum_tg += Tk * bx * (c - P.h);
+      sum_qc += q * c;
+      vx += q * bk.ux;
+      vy += q * bk.uy;
+      vz += q * bk.uz;
+    }
+    const T m = T(-2) * fcj / bj.d;
+    const T radial = T(0.5) * (sA[sj] - dfcj * sum_tg - m * sum_qc), perp = T(0.5) * m;
+    fx[sj] = radial * bj.ux + perp * vx;
+    fy[sj] = radial * bj.uy + perp * vy;
+    fz[sj] = radial * bj.uz + perp * vz;
+  }
+}
+
+// F_i = sum_j (f_ij - f_ji); the per-atom virial of the reference's output layout
+// (minimal_tersoff.cu:377-404): W_i,ab = -1/2 sum_j r_ij,a (f_ij - f_ji)_b in the order
+// xx, yy, zz, xy, yz, zx (not symmetrised).
+template <class T, class Lay>
+__global__ void plain_tersoff_gather(int N, Lay L, const int* __restrict__ rev, const double4* __restrict__ g,
+                                     const T* __restrict__ fx, const T* __restrict__ fy, const T* __restrict__ fz,
+                                     T* __restrict__ F, T* __restrict__ W) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  T f[3] = {T(0), T(0), T(0)}, w[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
   const int Z = L.count(i);
-  for (int k1 = 0; k1 < Z; ++k1) {
-    const int i1 = L.slot(i, k1);
-    const int n2 = L.nb(i, k1);
-    T x12, y12, z12, d12;
-    bond(g, i1, x12, y12, z12, d12);
-    T zeta = 0;
-    for (int k2 = 0; k2 < Z; ++k2) {
-      const int i2 = L.slot(i, k2);
-      if (L.nb(i, k2) == n2) continue;
-      T x13, y13, z13, d13;
-      bond(g, i2, x13, y13, z13, d13);
-      const T cs = (x12 * x13 + y12 * y13 + z12 * z13) / (d12 * d13);
-      T fc13, fcp13;
-      fcut(P.R1, P.R2, P.PF, d13, fc13, fcp13);
-      const T x = cs - P.H;
-      zeta += fc13 * P.BETA * x * x;
-    }
-    const T bzn = pow(zeta, P.EN);
-    const T bij = pow(T(1) + bzn, P.MHON);
-    if (zeta < T(1.0e-16)) {
-      b[i1] = 1;
-      bp[i1] = 0;
-    } else {
-      b[i1] = bij;
-      bp[i1] = -bij * bzn * T(0.5) / ((T(1) + bzn) * zeta);
+  for (int j = 0; j < Z; ++j) {
+    const int sj = L.slot(i, j), sr = rev[sj];
+    const double4 q = g[sj];
+    const T r[3] = {(T)q.x, (T)q.y, (T)q.z};
+    const T df[3] = {fx[sj] - fx[sr], fy[sj] - fy[sr], fz[sj] - fz[sr]};
+    for (int a = 0; a < 3; ++a) {
+      f[a] += df[a];
+      w[a] -= T(0.5) * r[a] * df[a];          // xx, yy, zz
+      w[3 + a] -= T(0.5) * r[a] * df[(a + 1) % 3];  // xy, yz, zx
     }
   }
+  for (int a = 0; a < 3; ++a) F[i + (size_t)a * N] = f[a];
+  for (int k = 0; k < 6; ++k) W[i + (size_t)k * N] = w[k];
 }
 
-// step 2 (minimal_tersoff.cu:191-316): partial forces and site energies
-template <class T, class Lay>
-__global__ void p_tersoff2(int N, int num_types, const int* __restrict__ type, Lay L,
-                           const double4* __restrict__ g, PT<T> P, const T* __restrict__ b,
-                           const T* __restrict__ bp, T* __restrict__ pe, T* __restrict__ fxs,
-                           T* __restrict__ fys, T* __restrict__ fzs) {
-  const int n1 = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n1 >= N) return;
-  const int type1 = type[n1];
-  const int Z = L.count(n1);
-  T pot = 0;
-  for (int k1 = 0; k1 < Z; ++k1) {
-    const int i1 = L.slot(n1, k1);
-    const int n2 = L.nb(n1, k1);
-    const int s12 = (num_types == 2 && type1 != type[n2]) ? 1 : 0;
-    T x12, y12, z12, d12;
-    bond(g, i1, x12, y12, z12, d12);
-    const T d12inv = T(1) / d12;
-    T fc12, fcp12;
-    fcut(P.R1, P.R2, P.PF, d12, fc12, fcp12);
-    const T lr = sqrt(T(2) * P.S[s12]) * P.A[s12], la = sqrt(T(2) / P.S[s12]) * P.A[s12];
-    const T fr12 = P.D0[s12] / (P.S[s12] - T(1)) * texp(-lr * (d12 - P.R0[s12]));
-    const T frp12 = -lr * fr12;
-    const T fa12 = P.S[s12] * P.D0[s12] / (P.S[s12] - T(1)) * texp(-la * (d12 - P.R0[s12]));
-    const T fap12 = -la * fa12;
-    const T b12 = b[i1];
-    const T factor3 = (fcp12 * (fr12 - b12 * fa12) + fc12 * (frp12 - b12 * fap12)) * d12inv;
-    T f12x = x12 * factor3 * T(0.5), f12y = y12 * factor3 * T(0.5), f12z = z12 * factor3 * T(0.5);
-    pot += fc12 * (fr12 - b12 * fa12) * T(0.5);
-    const T bp12 = bp[i1];
-    for (int k2 = 0; k2 < Z; ++k2) {
-      const int i2 = L.slot(n1, k2);
-      const int n3 = L.nb(n1, k2);
-      if (n3 == n2) continue;
-      const int s13 = (num_types == 2 && type1 != type[n3]) ? 1 : 0;
-      T x13, y13, z13, d13;
-      bond(g, i2, x13, y13, z13, d13);
-      T fc13, fcp13;
-      fcut(P.R1, P.R2, P.PF, d13, fc13, fcp13);
-      const T la13 = sqrt(T(2) / P.S[s13]) * P.A[s13];
-      const T fa13 = P.S[s13] * P.D0[s13] / (P.S[s13] - T(1)) * texp(-la13 * (d13 - P.R0[s13]));
-      const T bp13 = bp[i2];
-      const T one_over_d12d13 = T(1) / (d12 * d13);
-      const T cos123 = (x12 * x13 + y12 * y13 + z12 * z13) * one_over_d12d13;
-      const T cos123_over_d12d12 = cos123 * d12inv * d12inv;
-      const T xx = cos123 - P.H;
-      const T g123 = P.BETA * xx * xx, gp123 = P.BETA * T(2) * xx;
-      const T dc = -fc12 * bp12 * fa12 * fc13 * gp123 - fc12 * bp13 * fa13 * fc13 * gp123;
-      const T dr = -fcp12 * bp13 * fa13 * g123 * fc13 * d12inv;
-      T cos_d = x13 * one_over_d12d13 - x12 * cos123_over_d12d12;
-      f12x += (x12 * dr + dc * cos_d) * T(0.5);
-      cos_d = y13 * one_over_d12d13 - y12 * cos123_over_d12d12;
-      f12y += (y12 * dr + dc * cos_d) * T(0.5);
-      cos_d = z13 * one_over_d12d13 - z12 * cos123_over_d12d12;
-      f12z += (z12 * dr + dc * cos_d) * T(0.5);
-    }
-    fxs[i1] = f12x;
-    fys[i1] = f12y;
-    fzs[i1] = f12z;
-  }
-  pe[n1] = pot;
-}
-
-// step 3 (minimal_tersoff.cu:318-405): force gather and per-atom virial
-template <class T, class Lay>
-__global__ void p_tersoff3(int N, Lay L, const int* __restrict__ rev, const double4* __restrict__ g,
-                           const T* __restrict__ fxs, const T* __restrict__ fys, const T* __restrict__ fzs,
-                           T* __restrict__ F, T* __restrict__ W) {
-  const int n1 = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n1 >= N) return;
-  T sfx = 0, sfy = 0, sfz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vyz = 0, vzx = 0;
-  const int Z = L.count(n1);
-  for (int k1 = 0; k1 < Z; ++k1) {
-    const int i1 = L.slot(n1, k1);
-    T x12, y12, z12, d12;
-    bond(g, i1, x12, y12, z12, d12);
-    const int r = rev[i1];
-    const T dx = fxs[i1] - fxs[r], dy = fys[i1] - fys[r], dz = fzs[i1] - fzs[r];
-    sfx += dx;
-    sfy += dy;
-    sfz += dz;
-    vxx -= x12 * dx * T(0.5);
-    vyy -= y12 * dy * T(0.5);
-    vzz -= z12 * dz * T(0.5);
-    vxy -= x12 * dy * T(0.5);
-    vyz -= y12 * dz * T(0.5);
-    vzx -= z12 * dx * T(0.5);
-  }
-  F[n1] = sfx;
-  F[n1 + N] = sfy;
-  F[n1 + 2 * (size_t)N] = sfz;
-  W[n1] = vxx;
-  W[n1 + N] = vyy;
-  W[n1 + 2 * (size_t)N] = vzz;
-  W[n1 + 3 * (size_t)N] = vxy;
-  W[n1 + 4 * (size_t)N] = vyz;
-  W[n1 + 5 * (size_t)N] = vzx;
-}
-
+// --------------------------------------------------------------------------- pair models
+// Rigid-ion pair energy U(d) and dU/dd for pair type t (0 cation-cation, 1 cation-anion with
+// Morse, 2 anion-anion): A e^{-d/rho} - C/d^6 + qq (erfc(alpha d)/d - v_rc - dv_rc (d - rc)).
 template <class T>
-__device__ __forceinline__ void ri_p2f2(const PR<T>& q, int t, T d, T& p2, T& f2) {
-  const T alpha = T(0.2), alpha_sq = T(0.04), pif = T(0.225675833419103);
-  const T dsq = d * d, dinv = T(1) / d, dinv3 = dinv * dinv * dinv, dinv6 = dinv3 * dinv3, dinv7 = dinv6 * dinv;
-  const T ex = texp(-d * q.b[t]);
-  const T erfc_r = erfc(alpha * d) * dinv;
-  p2 = q.a[t] * ex - q.c[t] * dinv6;
-  f2 = T(6) * q.c[t] * dinv7 - q.a[t] * ex * q.b[t];
-  p2 += q.qq[t] * (erfc_r - q.v_rc - q.dv_rc * (d - q.cutoff));
-  f2 -= q.qq[t] * (erfc_r * dinv + pif * dinv * texp(-alpha_sq * dsq) + q.dv_rc);
+__device__ __forceinline__ void rigid_ion_pair(const RigidIon<T>& R, int t, T d, T& U, T& dU) {
+  const T id = T(1) / d, id6 = id * id * id * id * id * id;
+  const T buck = R.A[t] * m_exp(-d * R.inv_rho[t]);
+  const T coul = m_erfc(T(kAlpha) * d) * id;
+  U = buck - R.C[t] * id6 + R.qq[t] * (coul - R.v_rc - R.dv_rc * (d - R.rc));
+  dU = -R.inv_rho[t] * buck + T(6) * R.C[t] * id6 * id -
+       R.qq[t] * (coul * id + T(kTwoOverSqrtPi * kAlpha) * m_exp(T(-kAlpha * kAlpha) * d * d) * id + R.dv_rc);
   if (t == 1) {
-    const T fr = q.d0 / (q.s - T(1)) * texp(-sqrt(T(2) * q.s) * q.alpha * (d - q.r0));
-    const T frp = -sqrt(T(2) * q.s) * q.alpha * fr;
-    const T fa = q.s * q.d0 / (q.s - T(1)) * texp(-sqrt(T(2) / q.s) * q.alpha * (d - q.r0));
-    const T fap = -sqrt(T(2) / q.s) * q.alpha * fa;
-    p2 += fr - fa;
-    f2 += frp - fap;
+    const T x = d - R.r0;
+    const T rep = R.cr * m_exp(-R.lr * x), att = R.ca * m_exp(-R.la * x);
+    U += rep - att;
+    dU += R.la * att - R.lr * rep;
   }
-  f2 *= dinv;
 }
 
+// 1 -> n -> n -> 1 tanh network of the distance (nn2b.cu:49-78 parameter order: w0[n], b0[n],
+// W1[n][n] row-major, b1[n], w2[n], b2) and its derivative, forward mode.
 template <class T>
-__device__ void nn_p2f2(const T* __restrict__ w, int n, T d, T& p2, T& f2) {
-  T x1[32], y1[32];
-  for (int a = 0; a < n; ++a) {
-    x1[a] = tanh(w[a] * d - w[a + n]);
-    y1[a] = (T(1) - x1[a] * x1[a]) * w[a];
+__device__ __forceinline__ void mlp_pair(const T* __restrict__ w, int n, T d, T& U, T& dU) {
+  T h1[32], dh1[32];
+  for (int m = 0; m < n; ++m) {
+    h1[m] = m_tanh(w[m] * d - w[n + m]);
+    dh1[m] = (T(1) - h1[m] * h1[m]) * w[m];
   }
-  p2 = 0;
-  f2 = 0;
+  const T* W1 = w + 2 * n;
+  const T* b1 = W1 + n * n;
+  const T* w2 = b1 + n;
+  U = T(0);
+  dU = T(0);
   for (int a = 0; a < n; ++a) {
-    T x2 = 0, y2 = 0;
+    T z = T(0), dz = T(0);
     for (int m = 0; m < n; ++m) {
-      x2 += w[2 * n + a * n + m] * x1[m];
-      y2 += w[2 * n + a * n + m] * y1[m];
+      z += W1[a * n + m] * h1[m];
+      dz += W1[a * n + m] * dh1[m];
     }
-    x2 = tanh(x2 - w[n * (n + 2) + a]);
-    y2 *= T(1) - x2 * x2;
-    p2 += w[n * (n + 3) + a] * x2;
-    f2 += w[n * (n + 3) + a] * y2;
+    const T h2 = m_tanh(z - b1[a]);
+    U += w2[a] * h2;
+    dU += w2[a] * (T(1) - h2 * h2) * dz;
   }
-  p2 = p2 - w[n * (n + 4)];
+  U -= w2[n];
 }
 
-// ri.cu:112-189 / nn2b.cu:94-173
-template <class T, class Lay>
-__global__ void p_pair(int N, int kind, const int* __restrict__ type, Lay L, const double4* __restrict__ g, PR<T> q,
-                       const T* __restrict__ w, PN nn, T* __restrict__ F, T* __restrict__ W, T* __restrict__ pe) {
-  const int n1 = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n1 >= N) return;
-  T e = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vyz = 0, vzx = 0;
-  const int Z = L.count(n1);
-  for (int k1 = 0; k1 < Z; ++k1) {
-    const int i1 = L.slot(n1, k1);
-    T x12, y12, z12, d12;
-    bond(g, i1, x12, y12, z12, d12);
-    T p2, f2;
-    if (kind == 0) {
-      ri_p2f2(q, type[n1] + type[L.nb(n1, k1)], d12, p2, f2);
+// Owner-computes pair loop: every atom walks its full list.  pe_i = 1/2 sum_j U_ij,
+// F_i = sum_j dU_ij u_ij, W_i = -1/2 sum_j d_ij dU_ij u_ij (x) u_ij (reference order).
+// KIND 0 rigid ion, 1 NN 2-body.
+template <class T, int KIND, class Lay>
+__global__ void plain_pair(int N, const int* __restrict__ type, Lay L, const double4* __restrict__ g, RigidIon<T> R,
+                           const T* __restrict__ w, int n, MlpTaper tp, T* __restrict__ F, T* __restrict__ W,
+                           T* __restrict__ pe) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  T e = T(0), f[3] = {T(0), T(0), T(0)}, v[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+  const int Z = L.count(i);
+  for (int j = 0; j < Z; ++j) {
+    const Bond<T> bj(g[L.slot(i, j)]);
+    T U, dU;
+    if (KIND == 0) {
+      rigid_ion_pair(R, type[i] + type[L.nb(i, j)], bj.d, U, dU);
     } else {
-      nn_p2f2(w, nn.n, d12, p2, f2);
-      T fc, fcp;
-      fcut((T)nn.r1, (T)nn.r2, (T)nn.pf, d12, fc, fcp);
-      if (nn.consistent) {
-        f2 = (f2 * fc + p2 * fcp) / d12;
-        p2 *= fc;
-      } else {
-        p2 *= fc;
-        f2 = (f2 * fc + p2 * fcp) / d12;
-      }
+      T Uraw, dUraw, fc, dfc;
+      mlp_pair(w, n, bj.d, Uraw, dUraw);
+      taper((T)tp.r1, (T)tp.r2, (T)tp.pf, bj.d, fc, dfc);
+      U = Uraw * fc;
+      // nn2b.cu:147-148 tapers the energy before it enters the force term
+      dU = dUraw * fc + (tp.consistent ? Uraw : U) * dfc;
     }
-    fx += x12 * f2;
-    fy += y12 * f2;
-    fz += z12 * f2;
-    vxx -= x12 * x12 * f2 * T(0.5);
-    vyy -= y12 * y12 * f2 * T(0.5);
-    vzz -= z12 * z12 * f2 * T(0.5);
-    vxy -= x12 * y12 * f2 * T(0.5);
-    vyz -= y12 * z12 * f2 * T(0.5);
-    vzx -= z12 * x12 * f2 * T(0.5);
-    e += p2 * T(0.5);
+    const T u[3] = {bj.ux, bj.uy, bj.uz};
+    const T s = T(-0.5) * bj.d * dU;
+    for (int a = 0; a < 3; ++a) {
+      f[a] += dU * u[a];
+      v[a] += s * u[a] * u[a];
+      v[3 + a] += s * u[a] * u[(a + 1) % 3];
+    }
+    e += T(0.5) * U;
   }
-  F[n1] = fx;
-  F[n1 + N] = fy;
-  F[n1 + 2 * (size_t)N] = fz;
-  W[n1] = vxx;
-  W[n1 + N] = vyy;
-  W[n1 + 2 * (size_t)N] = vzz;
-  W[n1 + 3 * (size_t)N] = vxy;
-  W[n1 + 4 * (size_t)N] = vyz;
-  W[n1 + 5 * (size_t)N] = vzx;
-  if (kind == 0) e -= q.qq[type[n1] == 0 ? 0 : 2] * q.self;
-  pe[n1] = e;
+  if (KIND == 0) e -= R.qq[type[i] == 0 ? 0 : 2] * R.self;  // self energy K_C q_i^2 S(rc)
+  for (int a = 0; a < 3; ++a) F[i + (size_t)a * N] = f[a];
+  for (int k = 0; k < 6; ++k) W[i + (size_t)k * N] = v[k];
+  pe[i] = e;
 }
 
+// ----------------------------------------------------------------- per-individual fitness
 // One CTA per configuration: FP64 sums of site energies / virials and of the
 // squared force error, then one thread folds them into the fitness
 // (fitness.cu:392-555 with FP64 accumulation).
@@ -374,56 +421,16 @@ __global__ void p_fitness(int Nc, const double* __restrict__ cfg, double nF, dou
 
 namespace {
 
-template <class T>
-PT<T> tersoff_consts(const float* p, int num_types) {
-  PT<T> t;
-  t.D0[0] = p[0]; t.A[0] = p[1]; t.R0[0] = p[2]; t.S[0] = p[3];
-  int off = 0;
-  if (num_types == 2) {
-    off = 4;
-    t.D0[1] = p[4]; t.A[1] = p[5]; t.R0[1] = p[6]; t.S[1] = p[7];
-  } else {
-    t.D0[1] = t.D0[0]; t.A[1] = t.A[0]; t.R0[1] = t.R0[0]; t.S[1] = t.S[0];
-  }
-  t.EN = p[4 + off];
-  t.BETA = p[5 + off];
-  t.H = p[6 + off];
-  t.R1 = p[7 + off];
-  t.R2 = p[8 + off];
-  t.PF = (T)(M_PI / ((double)t.R2 - (double)t.R1));
-  t.MHON = (T)(-0.5 / (double)t.EN);
-  return t;
-}
-
-template <class T>
-PR<T> ri_consts(const float* p, int potential_type, bool with_self) {
-  PR<T> r;
-  const double q0 = p[0], kc = 14.399645, alpha = 0.2, pif = 0.225675833419103;
-  const double ratio = ri_charge_ratio(potential_type);
-  r.qq[0] = (T)(q0 * q0 * kc);
-  r.qq[1] = (T)(ratio * q0 * q0 * kc);
-  r.qq[2] = (T)(ratio * ratio * q0 * q0 * kc);
-  for (int t = 0; t < 3; ++t) {
-    r.a[t] = p[1 + 3 * t];
-    r.b[t] = (T)(1.0 / (double)p[2 + 3 * t]);
-    r.c[t] = p[3 + 3 * t];
-  }
-  const double rc = p[10];
-  r.cutoff = (T)rc;
-  r.d0 = p[11];
-  r.alpha = p[12];
-  r.r0 = p[13];
-  r.s = p[14];
-  r.v_rc = (T)(erfc(alpha * rc) / rc);
-  r.dv_rc = (T)(-erfc(alpha * rc) / (rc * rc) - pif * exp(-alpha * alpha * rc * rc) / rc);
-  r.self = with_self ? (T)ri_self_factor(rc) : T(0);
-  return r;
-}
-
+// Device buffers of one evaluation: per-bond scratch (S, A, f_ij x/y/z), per-atom outputs.
 template <class T>
 struct Scratch {
-  T *b, *bp, *fx, *fy, *fz, *F, *W, *pe, *w;
+  T *S, *A, *fx, *fy, *fz, *F, *W, *pe;
 };
+
+template <class T>
+Scratch<T> carve(T* bonds, size_t B, T* F, T* W, T* pe) {
+  return Scratch<T>{bonds, bonds + B, bonds + 2 * B, bonds + 3 * B, bonds + 4 * B, F, W, pe};
+}
 
 template <class T>
 int ensure_scratch(Engine* e, Scratch<T>* s);
@@ -432,13 +439,12 @@ template <>
 int ensure_scratch<double>(Engine* e, Scratch<double>* s) {
   const size_t B = std::max(e->d.B, 1), N = e->d.N;
   if (!e->s64) {
-    GPUGA_TRY(e->alloc(&e->s64, 5 * B + (size_t)std::max(e->d.num_vars, 1)));
+    GPUGA_TRY(e->alloc(&e->s64, 5 * B));
     GPUGA_TRY(e->alloc(&e->p64_F, 3 * N));
     GPUGA_TRY(e->alloc(&e->p64_W, 6 * N));
     GPUGA_TRY(e->alloc(&e->p64_pe, N));
   }
-  *s = {e->s64, e->s64 + B, e->s64 + 2 * B, e->s64 + 3 * B, e->s64 + 4 * B, e->p64_F, e->p64_W, e->p64_pe,
-        e->s64 + 5 * B};
+  *s = carve(e->s64, B, e->p64_F, e->p64_W, e->p64_pe);
   return GPUGA_OK;
 }
 
@@ -446,47 +452,63 @@ template <>
 int ensure_scratch<float>(Engine* e, Scratch<float>* s) {
   const size_t B = std::max(e->d.B, 1), N = e->d.N;
   if (!e->s32) {
-    GPUGA_TRY(e->alloc(&e->s32, 5 * B + (size_t)std::max(e->d.num_vars, 1)));
+    GPUGA_TRY(e->alloc(&e->s32, 5 * B));
     GPUGA_TRY(e->alloc(&e->p32_F, 3 * N));
     GPUGA_TRY(e->alloc(&e->p32_W, 6 * N));
     GPUGA_TRY(e->alloc(&e->p32_pe, N));
   }
-  *s = {e->s32, e->s32 + B, e->s32 + 2 * B, e->s32 + 3 * B, e->s32 + 4 * B, e->p32_F, e->p32_W, e->p32_pe,
-        e->s32 + 5 * B};
+  *s = carve(e->s32, B, e->p32_F, e->p32_W, e->p32_pe);
   return GPUGA_OK;
 }
 
-// Enqueues the force launches of one individual (decoded FP32 parameters).
-template <class T>
-int enqueue_force(Engine* e, const float* params, const Scratch<T>& s, cudaStream_t st) {
-  const DevSet& d = e->d;
-  const int N = d.N, grid = (N + 127) / 128;
-  if (d.potential_type == 1 || d.potential_type == 2) {
-    const PT<T> P = tersoff_consts<T>(params, d.num_types);
-    const CsrLayout L{d.off, d.nbr};
-    p_tersoff1<T><<<grid, 128, 0, st>>>(N, L, d.g64, P, s.b, s.bp);
-    p_tersoff2<T><<<grid, 128, 0, st>>>(N, d.num_types, d.type, L, d.g64, P, s.b, s.bp, s.pe, s.fx, s.fy, s.fz);
-    p_tersoff3<T><<<grid, 128, 0, st>>>(N, L, d.rev, d.g64, s.fx, s.fy, s.fz, s.F, s.W);
-  } else {
-    PR<T> q{};
-    PN nn{d.num_neurons, e->spec.nn_r1, e->spec.nn_r2, M_PI / ((double)e->spec.nn_r2 - e->spec.nn_r1),
-          e->spec.nn_consistent};
-    if (is_ri_type(d.potential_type)) {
-      q = ri_consts<T>(params, d.potential_type, e->spec.ri_self != 0);
-    } else {
-      if (d.num_neurons > 32) {
-        set_error("the plain NN2B path supports up to 32 neurons per layer.");
-        return GPUGA_ERR_UNSUPPORTED;
-      }
-      std::vector<T> w(d.num_vars);
-      for (int m = 0; m < d.num_vars; ++m) w[m] = params[m];
-      GPUGA_CUDA(cudaMemcpyAsync(s.w, w.data(), sizeof(T) * d.num_vars, cudaMemcpyHostToDevice, st));
-      GPUGA_CUDA(cudaStreamSynchronize(st));  // w is a stack buffer
+MlpTaper mlp_taper(const PotentialSpec& sp) {
+  return MlpTaper{sp.nn_r1, sp.nn_r2, M_PI / ((double)sp.nn_r2 - sp.nn_r1), sp.nn_consistent};
+}
+
+// Enqueues the force launches of one parameter vector p (decoded, FP64) on `st`.  NN2B reads its
+// weights from the device array w (already in T).
+template <class T, class Lay>
+int enqueue_force(int potential_type, int num_neurons, const double* p, const PotentialSpec& sp, int N,
+                  const int* type, Lay L, const int* rev, const double4* g, const T* w, const Scratch<T>& s,
+                  cudaStream_t st) {
+  const int grid = (N + 127) / 128;
+  if (potential_type == 1 || potential_type == 2) {
+    const int num_types = potential_type == 2 ? 2 : 1;
+    const TersoffSet<T> P = tersoff_set<T>(p, num_types);
+    plain_tersoff_bonds<T><<<grid, 128, 0, st>>>(N, num_types, type, L, g, P, s.S, s.A, s.fx, s.fy, s.fz, s.pe);
+    plain_tersoff_gather<T><<<grid, 128, 0, st>>>(N, L, rev, g, s.fx, s.fy, s.fz, s.F, s.W);
+  } else if (is_ri_type(potential_type)) {
+    const RigidIon<T> R = rigid_ion_set<T>(p, potential_type, sp.ri_self != 0);
+    plain_pair<T, 0><<<grid, 128, 0, st>>>(N, type, L, g, R, nullptr, 0, MlpTaper{}, s.F, s.W, s.pe);
+  } else if (potential_type == 3) {
+    if (num_neurons < 1 || num_neurons > 32) {
+      set_error("the plain NN2B path supports 1 to 32 neurons per layer (got %d).", num_neurons);
+      return GPUGA_ERR_UNSUPPORTED;
     }
-    p_pair<T><<<grid, 128, 0, st>>>(N, is_ri_type(d.potential_type) ? 0 : 1, d.type, CsrLayout{d.off, d.nbr}, d.g64, q,
-                                    s.w, nn, s.F, s.W, s.pe);
+    plain_pair<T, 1><<<grid, 128, 0, st>>>(N, type, L, g, RigidIon<T>{}, w, num_neurons, mlp_taper(sp), s.F, s.W,
+                                           s.pe);
+  } else {
+    set_error("unsupported potential type %d.", potential_type);
+    return GPUGA_ERR_UNSUPPORTED;
   }
   GPUGA_CUDA(cudaGetLastError());
+  return GPUGA_OK;
+}
+
+// Device copy of P parameter vectors in T for NN2B (the kernels read weights from HBM).
+template <class T>
+int upload_weights(Engine* e, const std::vector<double>& host, T** out) {
+  const size_t need = host.size() * sizeof(T);
+  if (e->p_w_bytes < need) {
+    if (e->p_w) cudaFree(e->p_w);
+    e->p_w = nullptr;
+    e->p_w_bytes = 0;
+    GPUGA_CUDA(cudaMalloc(&e->p_w, need));
+    e->p_w_bytes = need;
+  }
+  std::vector<T> conv(host.begin(), host.end());
+  GPUGA_CUDA(cudaMemcpy(e->p_w, conv.data(), need, cudaMemcpyHostToDevice));
+  *out = static_cast<T*>(e->p_w);
   return GPUGA_OK;
 }
 
@@ -495,6 +517,7 @@ int plain_fitness_t(Engine* e, int P, const float* pop01, double* fitness, doubl
   Scratch<T> s;
   GPUGA_TRY(ensure_scratch<T>(e, &s));
   const DevSet& d = e->d;
+  const int nv = d.num_vars;
   cudaStream_t st = e->stream;
   if (e->p_out_cap < P) {
     if (e->p_out) cudaFree(e->p_out);
@@ -503,10 +526,19 @@ int plain_fitness_t(Engine* e, int P, const float* pop01, double* fitness, doubl
     e->p_out_cap = P;
   }
   double* cfg = e->p_out + 4 * (size_t)P;
-  std::vector<float> params(d.num_vars);
+  // FP32 decode as the reference does (fitness.cu:320-324), then the individual's parameters in T
+  std::vector<double> params((size_t)P * nv);
+  std::vector<float> p32(nv);
   for (int p = 0; p < P; ++p) {
-    decode_params(e->spec, pop01 + (size_t)p * d.num_vars, params.data());
-    GPUGA_TRY(enqueue_force<T>(e, params.data(), s, st));
+    decode_params(e->spec, pop01 + (size_t)p * nv, p32.data());
+    for (int m = 0; m < nv; ++m) params[(size_t)p * nv + m] = p32[m];
+  }
+  T* w = nullptr;
+  if (d.potential_type == 3) GPUGA_TRY(upload_weights<T>(e, params, &w));
+  const CsrLayout L{d.off, d.nbr};
+  for (int p = 0; p < P; ++p) {
+    GPUGA_TRY(enqueue_force<T>(d.potential_type, d.num_neurons, params.data() + (size_t)p * nv, e->spec, d.N, d.type,
+                               L, d.rev, d.g64, w ? w + (size_t)p * nv : nullptr, s, st));
     p_config_errors<T><<<d.Nc, 256, 0, st>>>(d.N, d.Nc, d.Nc_force, d.Na, d.Na_sum, s.F, s.W, s.pe, d.force_ref,
                                              d.E_ref, d.W_ref, cfg);
     p_fitness<<<1, 32, 0, st>>>(d.Nc, cfg, d.norm_force, d.norm_energy, d.norm_virial, d.w_force, d.w_energy,
@@ -524,6 +556,25 @@ int plain_fitness_t(Engine* e, int P, const float* pop01, double* fitness, doubl
   return GPUGA_OK;
 }
 
+// One parameter vector on the engine's training set; outputs copied to the host.
+template <class T>
+int plain_find_force_t(Engine* e, const std::vector<double>& params, T* F, T* W, T* pe) {
+  Scratch<T> s;
+  GPUGA_TRY(ensure_scratch<T>(e, &s));
+  const DevSet& d = e->d;
+  cudaStream_t st = e->stream;
+  T* w = nullptr;
+  if (d.potential_type == 3) GPUGA_TRY(upload_weights<T>(e, params, &w));
+  GPUGA_TRY(enqueue_force<T>(d.potential_type, d.num_neurons, params.data(), e->spec, d.N, d.type,
+                             CsrLayout{d.off, d.nbr}, d.rev, d.g64, w, s, st));
+  const size_t N = d.N;
+  if (F) GPUGA_CUDA(cudaMemcpyAsync(F, s.F, sizeof(T) * 3 * N, cudaMemcpyDeviceToHost, st));
+  if (W) GPUGA_CUDA(cudaMemcpyAsync(W, s.W, sizeof(T) * 6 * N, cudaMemcpyDeviceToHost, st));
+  if (pe) GPUGA_CUDA(cudaMemcpyAsync(pe, s.pe, sizeof(T) * N, cudaMemcpyDeviceToHost, st));
+  GPUGA_CUDA(cudaStreamSynchronize(st));
+  return GPUGA_OK;
+}
+
 }  // namespace
 
 int plain_fitness(Engine* e, bool fp64, int P, const float* pop01, double* fitness, double* comps) {
@@ -531,89 +582,13 @@ int plain_fitness(Engine* e, bool fp64, int P, const float* pop01, double* fitne
               : plain_fitness_t<float>(e, P, pop01, fitness, comps);
 }
 
+// FP64 parameters stay exact: the constants are derived from them directly.
 int plain_find_force64(Engine* e, const double* params, double* F, double* W, double* pe) {
-  Scratch<double> s;
-  GPUGA_TRY(ensure_scratch<double>(e, &s));
-  // The FP64 path takes FP64 parameters: keep them exact by going through the
-  // double constants directly.
-  const DevSet& d = e->d;
-  cudaStream_t st = e->stream;
-  const int N = d.N, grid = (N + 127) / 128;
-  if (d.potential_type == 1 || d.potential_type == 2) {
-    PT<double> P;
-    P.D0[0] = params[0]; P.A[0] = params[1]; P.R0[0] = params[2]; P.S[0] = params[3];
-    int off = 0;
-    if (d.num_types == 2) {
-      off = 4;
-      P.D0[1] = params[4]; P.A[1] = params[5]; P.R0[1] = params[6]; P.S[1] = params[7];
-    } else {
-      P.D0[1] = P.D0[0]; P.A[1] = P.A[0]; P.R0[1] = P.R0[0]; P.S[1] = P.S[0];
-    }
-    P.EN = params[4 + off];
-    P.BETA = params[5 + off];
-    P.H = params[6 + off];
-    P.R1 = params[7 + off];
-    P.R2 = params[8 + off];
-    P.PF = M_PI / (P.R2 - P.R1);
-    P.MHON = -0.5 / P.EN;
-    const CsrLayout L{d.off, d.nbr};
-    p_tersoff1<double><<<grid, 128, 0, st>>>(N, L, d.g64, P, s.b, s.bp);
-    p_tersoff2<double><<<grid, 128, 0, st>>>(N, d.num_types, d.type, L, d.g64, P, s.b, s.bp, s.pe, s.fx, s.fy,
-                                             s.fz);
-    p_tersoff3<double><<<grid, 128, 0, st>>>(N, L, d.rev, d.g64, s.fx, s.fy, s.fz, s.F, s.W);
-  } else {
-    PR<double> q{};
-    PN nn{d.num_neurons, e->spec.nn_r1, e->spec.nn_r2, M_PI / ((double)e->spec.nn_r2 - e->spec.nn_r1),
-          e->spec.nn_consistent};
-    if (is_ri_type(d.potential_type)) {
-      const double q0 = params[0], kc = 14.399645, alpha = 0.2, pif = 0.225675833419103;
-      const double ratio = ri_charge_ratio(d.potential_type);
-      q.qq[0] = q0 * q0 * kc;
-      q.qq[1] = ratio * q0 * q0 * kc;
-      q.qq[2] = ratio * ratio * q0 * q0 * kc;
-      for (int t = 0; t < 3; ++t) {
-        q.a[t] = params[1 + 3 * t];
-        q.b[t] = 1.0 / params[2 + 3 * t];
-        q.c[t] = params[3 + 3 * t];
-      }
-      q.cutoff = params[10];
-      q.d0 = params[11];
-      q.alpha = params[12];
-      q.r0 = params[13];
-      q.s = params[14];
-      q.v_rc = erfc(alpha * q.cutoff) / q.cutoff;
-      q.dv_rc = -erfc(alpha * q.cutoff) / (q.cutoff * q.cutoff) -
-                pif * exp(-alpha * alpha * q.cutoff * q.cutoff) / q.cutoff;
-      q.self = e->spec.ri_self ? ri_self_factor(q.cutoff) : 0.0;
-    } else {
-      if (d.num_neurons > 32) {
-        set_error("the plain NN2B path supports up to 32 neurons per layer.");
-        return GPUGA_ERR_UNSUPPORTED;
-      }
-      GPUGA_CUDA(cudaMemcpyAsync(s.w, params, sizeof(double) * d.num_vars, cudaMemcpyHostToDevice, st));
-    }
-    p_pair<double><<<grid, 128, 0, st>>>(N, is_ri_type(d.potential_type) ? 0 : 1, d.type, CsrLayout{d.off, d.nbr}, d.g64,
-                                         q, s.w, nn, s.F, s.W, s.pe);
-  }
-  GPUGA_CUDA(cudaGetLastError());
-  if (F) GPUGA_CUDA(cudaMemcpyAsync(F, s.F, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st));
-  if (W) GPUGA_CUDA(cudaMemcpyAsync(W, s.W, sizeof(double) * 6 * N, cudaMemcpyDeviceToHost, st));
-  if (pe) GPUGA_CUDA(cudaMemcpyAsync(pe, s.pe, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
-  GPUGA_CUDA(cudaStreamSynchronize(st));
-  return GPUGA_OK;
+  return plain_find_force_t<double>(e, std::vector<double>(params, params + e->d.num_vars), F, W, pe);
 }
 
 int plain_find_force32(Engine* e, const float* params, float* F, float* W, float* pe) {
-  Scratch<float> s;
-  GPUGA_TRY(ensure_scratch<float>(e, &s));
-  cudaStream_t st = e->stream;
-  const int N = e->d.N;
-  GPUGA_TRY(enqueue_force<float>(e, params, s, st));
-  if (F) GPUGA_CUDA(cudaMemcpyAsync(F, s.F, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, st));
-  if (W) GPUGA_CUDA(cudaMemcpyAsync(W, s.W, sizeof(float) * 6 * N, cudaMemcpyDeviceToHost, st));
-  if (pe) GPUGA_CUDA(cudaMemcpyAsync(pe, s.pe, sizeof(float) * N, cudaMemcpyDeviceToHost, st));
-  GPUGA_CUDA(cudaStreamSynchronize(st));
-  return GPUGA_OK;
+  return plain_find_force_t<float>(e, std::vector<double>(params, params + e->d.num_vars), F, W, pe);
 }
 
 // --------------------------------------------------------------- reference-layout Potential
@@ -626,49 +601,27 @@ size_t ref_potential_scratch_bytes(int potential_type, int num_neurons, int N, i
 }
 
 // Potential::find_force (potential.cuh:28-40) in FP32 on the reference's
-// layouts: bond geometry from the FP32 image rule, then the three Tersoff steps
-// or the pair loop, all enqueued on `st`; nothing is allocated here.
+// layouts: bond geometry from the FP32 image rule, then the Tersoff passes or
+// the pair loop, all enqueued on `st`; nothing is allocated here.  `params` is a
+// host array (decoded parameters in potential.in order); NN2B weights are copied
+// from it into the scratch.
 int ref_potential_find_force(int potential_type, int num_neurons, const float* params, const PotentialSpec& nn_opts,
                              int Nc, int N, const int* Na, const int* Na_sum, int max_Na, const int* type,
                              const float* h, const int* NN, const int* NL, const float* r, float* f, float* virial,
                              float* pe, const RefPotentialScratch& s, cudaStream_t st) {
-  (void)max_Na;
-  GPUGA_TRY(ref_layout_geometry(Nc, N, Na, Na_sum, h, r, NN, NL, s.g64, s.rev, st));
-  const size_t slots = (size_t)N * (size_t)max_Na;
-  float* b = s.f5;
-  float* bp = s.f5 + slots;
-  float* fx = s.f5 + 2 * slots;
-  float* fy = s.f5 + 3 * slots;
-  float* fz = s.f5 + 4 * slots;
-  const RefLayout L{N, NN, NL};
-  const int grid = (N + 127) / 128;
-  if (potential_type == 1 || potential_type == 2) {
-    const int num_types = potential_type == 2 ? 2 : 1;
-    const PT<float> P = tersoff_consts<float>(params, num_types);
-    p_tersoff1<float><<<grid, 128, 0, st>>>(N, L, s.g64, P, b, bp);
-    p_tersoff2<float><<<grid, 128, 0, st>>>(N, num_types, type, L, s.g64, P, b, bp, pe, fx, fy, fz);
-    p_tersoff3<float><<<grid, 128, 0, st>>>(N, L, s.rev, s.g64, fx, fy, fz, f, virial);
-  } else if (is_ri_type(potential_type) || potential_type == 3) {
-    PR<float> q{};
-    PN nn{num_neurons, nn_opts.nn_r1, nn_opts.nn_r2, M_PI / ((double)nn_opts.nn_r2 - nn_opts.nn_r1),
-          nn_opts.nn_consistent};
-    if (is_ri_type(potential_type)) {
-      q = ri_consts<float>(params, potential_type, nn_opts.ri_self != 0);
-    } else {
-      if (num_neurons > 32) {
-        set_error("the NN2B Potential entry points support up to 32 neurons per layer.");
-        return GPUGA_ERR_UNSUPPORTED;
-      }
-      GPUGA_CUDA(cudaMemcpyAsync(s.w, params, sizeof(float) * num_vars_for(3, num_neurons), cudaMemcpyHostToDevice,
-                                 st));
-    }
-    p_pair<float><<<grid, 128, 0, st>>>(N, is_ri_type(potential_type) ? 0 : 1, type, L, s.g64, q, s.w, nn, f, virial, pe);
-  } else {
+  const int nv = num_vars_for(potential_type, num_neurons);
+  if (nv < 0) {
     set_error("unsupported potential type %d.", potential_type);
     return GPUGA_ERR_UNSUPPORTED;
   }
-  GPUGA_CUDA(cudaGetLastError());
-  return GPUGA_OK;
+  GPUGA_TRY(ref_layout_geometry(Nc, N, Na, Na_sum, h, r, NN, NL, s.g64, s.rev, st));
+  const size_t slots = (size_t)N * (size_t)max_Na;
+  Scratch<float> sc{s.f5, s.f5 + slots, s.f5 + 2 * slots, s.f5 + 3 * slots, s.f5 + 4 * slots, f, virial, pe};
+  if (potential_type == 3 && num_neurons >= 1 && num_neurons <= 32)
+    GPUGA_CUDA(cudaMemcpyAsync(s.w, params, sizeof(float) * nv, cudaMemcpyHostToDevice, st));
+  const std::vector<double> p(params, params + nv);
+  return enqueue_force<float>(potential_type, num_neurons, p.data(), nn_opts, N, type, RefLayout{N, NN, NL}, s.rev,
+                              s.g64, s.w, sc, st);
 }
 
 }  // namespace gpuga

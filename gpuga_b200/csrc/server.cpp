@@ -1,22 +1,37 @@
 // Serving loop: many fitting jobs on one GPU with continuous batching.
 //
-// A scheduler thread owns the device.  Jobs are admitted in arrival order as
-// long as the sum of their device footprints stays within the HBM budget and
-// the number of resident jobs is below max_jobs; every resident job keeps its
-// training set, population and GA buffers and per-(individual, configuration)
-// results on the GPU.  The scheduler advances all resident jobs together in
-// windows of up to kWindow generations.  Each generation is one CUDA graph: a
-// single launch set (one decode, the shared batched force launches whose work
-// items come from all jobs, one fitness fold) evaluates every job's
-// population, then the batched GA kernels (ga_device.cu) select, cross over
-// and mutate every job's population from random choices the host drew for the
-// window in advance -- no population or fitness crosses PCIe between
-// generations.  Jobs that arrive while others run join at the next window
-// boundary; finished or cancelled jobs leave and free their memory.  Work
-// items of different jobs never share a CTA and all reductions are
+// Three kinds of work, two host threads.
+//
+//   Loader thread.  Admits queued jobs in arrival order while the sum of their
+//   device footprints stays within the HBM budget and fewer than max_jobs are
+//   loading, ready or running: parses nothing (submit did), builds the engine
+//   (training set upload, neighbor lists, geometry), the population plan, the
+//   host GA (seeded RNG stream) and the device GA buffers, uploads the initial
+//   population and hands the job to the scheduler as "ready".  It also frees
+//   the device memory of finished jobs and of retired launch sets, so that no
+//   cudaFree (which waits for the device) runs on the scheduler thread.
+//
+//   Scheduler thread.  Owns one stream and runs all resident jobs together in
+//   windows of up to kWindow generations.  Each generation is one CUDA graph:
+//   one launch set (one decode, the shared batched force launches whose work
+//   items come from all jobs, one fitness fold) evaluates every job's
+//   population, then the batched GA kernels (ga_device.cu) select, cross over
+//   and mutate every job's population from random choices the host drew for
+//   the window in advance -- no population or fitness crosses PCIe between
+//   generations.  Windows are pipelined: while window k runs, the scheduler
+//   decides window k + 1's members (jobs that still have generations left plus
+//   every ready job), rebuilds the launch set and GA batch if they changed,
+//   draws and uploads the next plans into the other plan buffer and enqueues
+//   window k + 1 behind window k; only then does it wait for window k and
+//   harvest its generation histories.
+//
+// Work items of different jobs never share a CTA and all reductions are
 // fixed-order, so a job's trajectory is identical alone and in any mix.
-// There is no counterpart in the reference, which fits one potential per
-// process (main.cu:25-55).
+// Latency is reported two ways: the device time of each generation of all
+// resident jobs, and per job and generation the wall-clock time between the
+// job's successive window harvests divided by the window's generations (every
+// stall -- rebuilds, admissions, frees -- included).  There is no counterpart
+// in the reference, which fits one potential per process (main.cu:25-55).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -62,10 +77,11 @@ struct Job {
   GA ga;                            // host side: random stream and plan draws
   std::unique_ptr<DeviceGA, void (*)(DeviceGA*)> dga{nullptr, device_ga_free};
   int gens_total = 0;
+  int gens_queued = 0;              // generations enqueued on the device (>= ga.generation)
   std::vector<float> best;
   std::vector<float> elite;
   bool cancel_requested = false;
-  Clock::time_point t_submit, t_start, t_end;
+  Clock::time_point t_submit, t_start, t_end, t_mark;
 };
 
 // Admission estimate of a training set's device footprint: per atom ~64 B,
@@ -85,9 +101,31 @@ size_t estimate_bytes(const PotentialSpec& spec, const TrainingSet& ts, int P) {
     trip += na * z * z;
   }
   const bool tersoff = spec.type == 1 || spec.type == 2;
-  double bytes = 64.0 * ts.N + 80.0 * bonds + (tersoff ? 4.0 * trip : 0.0);
+  double bytes = 64.0 * ts.N + 88.0 * bonds + (tersoff ? 4.0 * trip : 0.0);
   bytes += (double)P * ts.Nc * kResK * 8.0 + (double)P * (spec.num_vars + 40) * 8.0;
   return (size_t)(1.25 * bytes) + (8u << 20);
+}
+
+// A resident set's shared launches and GA batch.
+struct Batch {
+  std::vector<Job*> jobs;
+  std::unique_ptr<LaunchSet> ls;
+  std::unique_ptr<GABatch, void (*)(GABatch*)> gab{nullptr, ga_batch_free};
+};
+
+// A window enqueued on the scheduler's stream.
+struct Window {
+  Batch* batch = nullptr;
+  int b = 0;   // plan buffer
+  int n = 0;   // generations
+};
+
+double percentile(std::vector<double> t, double q) {
+  if (t.empty()) return 0.0;
+  std::sort(t.begin(), t.end());
+  const double pos = q * (t.size() - 1);
+  const size_t lo = (size_t)std::floor(pos), hi = (size_t)std::ceil(pos);
+  return t[lo] + (t[hi] - t[lo]) * (pos - lo);
 }
 
 }  // namespace
@@ -101,182 +139,260 @@ struct gpuga_server {
   double budget = 0;
   int max_jobs = 0;
   std::mutex mu;
-  std::condition_variable cv;       // wakes the scheduler
-  std::condition_variable idle_cv;  // wakes drain()
-  std::deque<Job*> queue;
-  std::vector<Job*> running;
+  std::condition_variable cv;         // wakes the scheduler
+  std::condition_variable loader_cv;  // wakes the loader
+  std::condition_variable idle_cv;    // wakes drain()
+  std::deque<Job*> queue;             // submitted, not yet taken by the loader
+  int loading = 0;                    // jobs the loader is setting up
+  std::vector<Job*> ready;            // set up, joining at the next window boundary
+  std::vector<Job*> running;          // members of the last enqueued window
+  std::vector<Job*> retiring;         // left with the window in flight, retired after it
+  std::vector<Job*> graveyard;        // finished jobs whose device memory the loader frees
+  std::vector<std::unique_ptr<Batch>> retired;  // launch sets no window uses any more
   std::map<int, std::unique_ptr<Job>> jobs;
   int next_id = 1;
   bool stop = false;
+  bool hold = false;                  // gpuga_server_hold: no new windows start
   size_t bytes_in_use = 0;
-  std::thread worker;
-  cudaStream_t st = nullptr;
-  std::unique_ptr<LaunchSet> ls;
-  std::unique_ptr<GABatch, void (*)(GABatch*)> gab{nullptr, ga_batch_free};
-  std::vector<int> ls_ids;
+  std::thread worker, loader;
+  cudaStream_t st = nullptr, st_copy = nullptr;
   // statistics
-  std::vector<double> tick_ms;  // device time of each generation (all resident jobs)
+  std::vector<double> tick_ms;   // device time of each generation of all resident jobs
+  std::vector<double> wall_ms;   // per job and generation: wall-clock time, stalls included
   long batches = 0, finished = 0;
   double evals = 0, busy_s = 0;
   int peak_resident = 0;
   int worker_status = GPUGA_OK;
 
   void run();
-  bool admit_locked(std::unique_lock<std::mutex>& lock);
-  int window();
+  void load();
+  int setup(Job* j);
+  int build_batch(const std::vector<Job*>& members, std::unique_ptr<Batch>* out);
+  int harvest(const Window& w);
   void finish(Job* j, int state, int status, const char* msg);
+  int resident() const { return loading + (int)ready.size() + (int)running.size(); }
 };
 
+// Marks a job finished (mu held); its device memory goes to the loader's graveyard.
 void gpuga_server::finish(Job* j, int state, int status, const char* msg) {
   j->state = state;
   j->status = status;
   if (msg) j->error = msg;
   j->t_end = Clock::now();
-  j->dga.reset();
-  j->plan_owner.reset();
-  j->plan = nullptr;
-  if (j->engine && !j->shared) delete j->engine;
-  j->engine = nullptr;
   bytes_in_use -= std::min(bytes_in_use, j->bytes);
   if (state == kDone) ++finished;
+  graveyard.push_back(j);
+  loader_cv.notify_all();
+  cv.notify_all();
+  idle_cv.notify_all();
 }
 
-// Moves queued jobs into the resident set while they fit (mu held).
-bool gpuga_server::admit_locked(std::unique_lock<std::mutex>& lock) {
-  bool changed = false;
-  while (!queue.empty() && (int)running.size() < max_jobs) {
-    Job* j = queue.front();
-    if (j->cancel_requested) {
-      queue.pop_front();
-      finish(j, kCancelled, GPUGA_ERR_CANCELLED, "cancelled before it started");
-      changed = true;
+// Loader thread work for one admitted job (mu not held).
+int gpuga_server::setup(Job* j) {
+  if (!j->engine) {
+    gpuga_options opt;
+    gpuga_default_options(&opt);
+    opt.device = device;
+    Engine* e = nullptr;
+    GPUGA_TRY(engine_create(j->spec, std::move(j->ts), opt, &e));
+    j->engine = e;
+  }
+  Plan* p = nullptr;
+  GPUGA_TRY(plan_build(j->engine, j->gp.population_size, &p));
+  j->plan_owner.reset(p);
+  j->plan = p;
+  GPUGA_TRY(j->ga.init(j->engine->spec.num_vars, j->engine->spec.pmin.data(), j->engine->spec.pmax.data(), j->gp,
+                       j->seed));
+  DeviceGA* g = nullptr;
+  GPUGA_TRY(device_ga_setup(j->ga, kWindow, &g));
+  j->dga.reset(g);
+  GPUGA_CUDA(cudaMemcpy(device_ga_population(g), j->ga.population.data(), sizeof(float) * j->ga.population.size(),
+                        cudaMemcpyHostToDevice));
+  return GPUGA_OK;
+}
+
+void gpuga_server::load() {
+  cudaSetDevice(device);
+  std::unique_lock<std::mutex> lock(mu);
+  while (true) {
+    if (!graveyard.empty() || !retired.empty()) {
+      std::vector<Job*> dead;
+      dead.swap(graveyard);
+      std::vector<std::unique_ptr<Batch>> old;
+      old.swap(retired);
+      lock.unlock();
+      old.clear();
+      for (Job* j : dead) {
+        j->dga.reset();
+        j->plan_owner.reset();
+        j->plan = nullptr;
+        if (j->engine && !j->shared) delete j->engine;
+        j->engine = nullptr;
+      }
+      lock.lock();
       continue;
     }
-    if ((double)(bytes_in_use + j->bytes) > budget && !running.empty()) break;  // wait for memory
-    queue.pop_front();
-    bytes_in_use += j->bytes;
-    j->state = kRunning;
-    j->t_start = Clock::now();
-    lock.unlock();
-    int s = GPUGA_OK;
-    if (!j->engine) {
-      gpuga_options opt;
-      gpuga_default_options(&opt);
-      opt.device = device;
-      Engine* e = nullptr;
-      s = engine_create(j->spec, std::move(j->ts), opt, &e);
-      if (s == GPUGA_OK) j->engine = e;
+    if (!queue.empty() && resident() < max_jobs) {
+      Job* j = queue.front();
+      if (j->cancel_requested) {
+        queue.pop_front();
+        finish(j, kCancelled, GPUGA_ERR_CANCELLED, "cancelled before it started");
+        continue;
+      }
+      if ((double)(bytes_in_use + j->bytes) <= budget || resident() == 0) {
+        queue.pop_front();
+        bytes_in_use += j->bytes;
+        ++loading;
+        lock.unlock();
+        const int s = setup(j);
+        lock.lock();
+        --loading;
+        if (s != GPUGA_OK) {
+          finish(j, kFailed, s, last_error());
+        } else if (j->cancel_requested) {
+          finish(j, kCancelled, GPUGA_ERR_CANCELLED, "cancelled before it started");
+        } else {
+          j->state = kRunning;
+          j->t_start = j->t_mark = Clock::now();
+          ready.push_back(j);
+          cv.notify_all();
+        }
+        continue;
+      }
     }
-    if (s == GPUGA_OK) {
-      Plan* p = nullptr;
-      s = plan_build(j->engine, j->gp.population_size, &p);
-      j->plan_owner.reset(p);
-      j->plan = p;
-    }
-    if (s == GPUGA_OK)
-      s = j->ga.init(j->engine->spec.num_vars, j->engine->spec.pmin.data(), j->engine->spec.pmax.data(), j->gp,
-                     j->seed);
-    if (s == GPUGA_OK) {
-      DeviceGA* g = nullptr;
-      s = device_ga_setup(j->ga, kWindow, &g);
-      j->dga.reset(g);
-    }
-    if (s == GPUGA_OK) {
-      const cudaError_t ce = cudaMemcpy(device_ga_population(j->dga.get()), j->ga.population.data(),
-                                        sizeof(float) * j->ga.population.size(), cudaMemcpyHostToDevice);
-      if (ce != cudaSuccess) s = cuda_status(ce, "cudaMemcpy", __FILE__, __LINE__);
-    }
-    lock.lock();
-    if (s != GPUGA_OK) {
-      finish(j, kFailed, s, last_error());
-    } else {
-      running.push_back(j);
-      peak_resident = std::max(peak_resident, (int)running.size());
-    }
-    changed = true;
+    if (stop && queue.empty()) break;
+    loader_cv.wait(lock);
   }
-  return changed;
 }
 
-// Up to kWindow generations of every resident job: shared fitness launches and
-// batched GA kernels per generation, one CUDA graph, no host round trip.
-int gpuga_server::window() {
-  std::vector<int> ids;
-  for (Job* j : running) ids.push_back(j->id);
-  if (!ls || ids != ls_ids) {
-    gab.reset();
-    std::vector<std::pair<Engine*, Plan*>> v;
-    std::vector<DeviceGA*> g;
-    for (Job* j : running) {
-      v.push_back({j->engine, j->plan});
-      g.push_back(j->dga.get());
-    }
-    ls.reset(new LaunchSet);
-    GPUGA_TRY(launchset_build(v, ls.get()));
-    for (size_t k = 0; k < running.size(); ++k)
-      GPUGA_TRY(launchset_retarget(ls.get(), (int)k, device_ga_population(g[k]), device_ga_fitness64(g[k]), nullptr,
-                                   st));
-    GABatch* b = nullptr;
-    GPUGA_TRY(ga_batch_build(g, ls.get(), &b));
-    gab.reset(b);
-    ls_ids = ids;
+// Launch set and GA batch of a resident set (host work plus small uploads; no wait on the device).
+int gpuga_server::build_batch(const std::vector<Job*>& members, std::unique_ptr<Batch>* out) {
+  std::unique_ptr<Batch> B(new Batch);
+  B->jobs = members;
+  std::vector<std::pair<Engine*, Plan*>> v;
+  std::vector<std::pair<const float*, double*>> targets;
+  std::vector<DeviceGA*> g;
+  for (Job* j : members) {
+    v.push_back({j->engine, j->plan});
+    targets.push_back({device_ga_population(j->dga.get()), device_ga_fitness64(j->dga.get())});
+    g.push_back(j->dga.get());
   }
-  int n = kWindow;
-  for (Job* j : running) n = std::min(n, j->gens_total - j->ga.generation);
-  if (n <= 0) return GPUGA_OK;
-  const auto t0 = Clock::now();
-  for (Job* j : running) {
-    device_ga_draw(j->ga, j->dga.get(), 0, j->ga.generation, n);
-    GPUGA_TRY(device_ga_upload(j->dga.get(), 0, n, st));
-  }
-  GPUGA_TRY(ga_batch_window(gab.get(), 0, n, true, true, st));
-  GPUGA_TRY(ga_batch_wait(gab.get(), 0));
+  B->ls.reset(new LaunchSet);
+  GPUGA_TRY(launchset_build(v, B->ls.get(), &targets));
+  GABatch* gb = nullptr;
+  GPUGA_TRY(ga_batch_build(g, B->ls.get(), &gb));
+  B->gab.reset(gb);
+  *out = std::move(B);
+  return GPUGA_OK;
+}
+
+// Waits for window w and records its results (mu not held; the jobs' run state is the
+// scheduler's own).
+int gpuga_server::harvest(const Window& w) {
+  GPUGA_TRY(ga_batch_wait(w.batch->gab.get(), w.b));
+  const auto now = Clock::now();
   std::vector<double> ms;
-  GPUGA_TRY(ga_batch_generation_ms(gab.get(), n, &ms));
-  for (Job* j : running) {
-    const float* h = device_ga_history(j->dga.get(), 0);
-    for (int q = 0; q < n; ++q) j->best.push_back(h[(size_t)q * (j->ga.d + 1)]);
-    j->ga.generation += n;
-    evals += (double)j->plan->P * j->engine->d.N * n;
+  GPUGA_TRY(ga_batch_generation_ms(w.batch->gab.get(), w.b, w.n, &ms));
+  std::lock_guard<std::mutex> g(mu);
+  for (Job* j : w.batch->jobs) {
+    const float* h = device_ga_history(j->dga.get(), w.b);
+    for (int q = 0; q < w.n; ++q) j->best.push_back(h[(size_t)q * (j->ga.d + 1)]);
+    j->ga.generation += w.n;
+    evals += (double)j->plan->P * j->engine->d.N * w.n;
+    const double per_gen = std::chrono::duration<double, std::milli>(now - j->t_mark).count() / w.n;
+    for (int q = 0; q < w.n; ++q) wall_ms.push_back(per_gen);
+    j->t_mark = now;
   }
-  // latency: device time of each generation; throughput: wall time of the window (plan draws,
-  // uploads and the history read-back included)
   for (double t : ms) tick_ms.push_back(t);
-  busy_s += std::chrono::duration<double>(Clock::now() - t0).count();
-  batches += n;
+  batches += w.n;
   return GPUGA_OK;
 }
 
 void gpuga_server::run() {
   cudaSetDevice(device);
-  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&st_copy, cudaStreamNonBlocking) != cudaSuccess) {
     std::lock_guard<std::mutex> g(mu);
     worker_status = GPUGA_ERR_CUDA;
     idle_cv.notify_all();
     return;
   }
+  std::unique_ptr<Batch> cur_batch;  // the launch set of the last enqueued window
+  Window cur;                        // in flight (cur.batch == nullptr: none)
+  Clock::time_point busy_since{};
+  int status = GPUGA_OK;
   std::unique_lock<std::mutex> lock(mu);
   while (true) {
-    admit_locked(lock);
-    if (running.empty()) {
+    // members of the next window: jobs with generations left after the one in flight, then
+    // every ready job (as many as the slots allow; the loader respects max_jobs already)
+    std::vector<Job*> next, leaving;
+    for (Job* j : running) {
+      if (status == GPUGA_OK && !j->cancel_requested && j->gens_queued < j->gens_total) next.push_back(j);
+      else leaving.push_back(j);
+    }
+    if (status == GPUGA_OK) {
+      for (Job* j : ready) next.push_back(j);
+      ready.clear();
+    }
+    if ((next.empty() || hold) && !cur.batch && leaving.empty()) {
+      running = next;  // held: loaded jobs wait here, no window starts
+      if (next.empty() && cur_batch) retired.push_back(std::move(cur_batch));
+      loader_cv.notify_all();
       idle_cv.notify_all();
-      if (stop) break;
+      if (stop && queue.empty() && loading == 0 && ready.empty() && running.empty()) break;
       cv.wait(lock);
       continue;
     }
+    const bool enqueue = !hold;
+    running = next;  // visible to drain() and poll() while the lock is released
+    retiring = leaving;
+    peak_resident = std::max(peak_resident, (int)next.size());
     lock.unlock();
-    const int s = window();
+    if (busy_since == Clock::time_point{} && !next.empty() && enqueue) busy_since = Clock::now();
+    // enqueue window k + 1 behind window k
+    Window nxt;
+    std::unique_ptr<Batch> next_batch;
+    if (!next.empty() && enqueue) {
+      int s = GPUGA_OK;
+      Batch* use = cur_batch.get();
+      if (!cur_batch || cur_batch->jobs != next) {
+        s = build_batch(next, &next_batch);
+        use = next_batch.get();
+      }
+      int n = kWindow;
+      for (Job* j : next) n = std::min(n, j->gens_total - j->gens_queued);
+      const int b = cur.batch ? cur.b ^ 1 : 0;
+      for (Job* j : next) {
+        if (s != GPUGA_OK) break;
+        device_ga_draw(j->ga, j->dga.get(), b, j->gens_queued, n);
+        s = device_ga_upload(j->dga.get(), b, n, st);
+      }
+      if (s == GPUGA_OK) s = ga_batch_window(use->gab.get(), b, n, true, true, st);
+      if (s == GPUGA_OK) {
+        nxt = Window{use, b, n};
+        for (Job* j : next) j->gens_queued += n;
+      } else {
+        status = s;
+      }
+    }
+    // then wait for window k
+    if (cur.batch && status == GPUGA_OK) status = harvest(cur);
+    if ((!nxt.batch || status != GPUGA_OK) && busy_since != Clock::time_point{}) {
+      // nothing follows: the busy period ends with window k
+      busy_s += std::chrono::duration<double>(Clock::now() - busy_since).count();
+      busy_since = Clock::time_point{};
+    }
     lock.lock();
-    // retire finished, failed and cancelled jobs at the window boundary
-    std::vector<Job*> keep;
-    for (Job* j : running) {
-      if (s != GPUGA_OK) {
-        finish(j, kFailed, s, last_error());
-      } else if (j->cancel_requested) {
-        finish(j, kCancelled, GPUGA_ERR_CANCELLED, "cancelled");
+    // retire the jobs that left with window k (finished, cancelled or failed)
+    for (Job* j : leaving) {
+      if (status != GPUGA_OK) {
+        finish(j, kFailed, status, last_error());
       } else if (j->ga.generation >= j->gens_total) {
-        // the final population (row 0 = the last generation's elite) comes back once
-        const int ss = device_ga_sync_host(&j->ga, j->dga.get(), 0, st);
+        // the final population (row 0 = the last generation's elite) comes back on a second
+        // stream: no later window touches this job's buffers
+        lock.unlock();
+        const int ss = device_ga_sync_host(&j->ga, j->dga.get(), 0, st_copy);
+        lock.lock();
         if (ss != GPUGA_OK) {
           finish(j, kFailed, ss, last_error());
           continue;
@@ -284,16 +400,29 @@ void gpuga_server::run() {
         j->elite.assign(j->ga.population.begin(), j->ga.population.begin() + j->ga.d);
         finish(j, kDone, GPUGA_OK, nullptr);
       } else {
-        keep.push_back(j);
+        finish(j, kCancelled, GPUGA_ERR_CANCELLED, "cancelled");
       }
     }
-    running.swap(keep);
-    if (s != GPUGA_OK) worker_status = s;
+    if (status != GPUGA_OK) {
+      worker_status = status;
+      for (Job* j : next) finish(j, kFailed, status, last_error());
+      next.clear();
+      nxt = Window{};
+    }
+    if (next_batch) {
+      if (cur_batch) retired.push_back(std::move(cur_batch));
+      cur_batch = std::move(next_batch);
+      loader_cv.notify_all();
+    }
+    running = next;
+    retiring.clear();
+    cur = nxt;
   }
-  gab.reset();
-  ls.reset();
+  lock.unlock();
+  cur_batch.reset();
   cudaStreamDestroy(st);
-  st = nullptr;
+  cudaStreamDestroy(st_copy);
+  st = st_copy = nullptr;
 }
 
 extern "C" {
@@ -314,6 +443,7 @@ int gpuga_server_create(int device, double hbm_budget_bytes, int max_jobs, gpuga
   s->budget = hbm_budget_bytes;
   s->max_jobs = max_jobs;
   s->worker = std::thread([s] { s->run(); });
+  s->loader = std::thread([s] { s->load(); });
   *out = s;
   return GPUGA_OK;
 }
@@ -331,7 +461,7 @@ static int enqueue_job(gpuga_server* s, std::unique_ptr<Job> j, int* job_id) {
   s->jobs[raw->id] = std::move(j);
   s->queue.push_back(raw);
   if (job_id) *job_id = raw->id;
-  s->cv.notify_all();
+  s->loader_cv.notify_all();
   return GPUGA_OK;
 }
 
@@ -390,7 +520,7 @@ int gpuga_server_poll(gpuga_server* s, int job_id, int* progress) {
   }
   Job* j = it->second.get();
   if (progress) {
-    progress[0] = j->state == kRunning || j->state == kDone ? j->ga.generation : 0;
+    progress[0] = j->state == kQueued ? 0 : j->ga.generation;  // cancelled / failed: generations run
     progress[1] = j->gens_total;
     progress[2] = j->state;
   }
@@ -433,6 +563,18 @@ int gpuga_server_cancel(gpuga_server* s, int job_id) {
   }
   it->second->cancel_requested = true;
   s->cv.notify_all();
+  s->loader_cv.notify_all();
+  return GPUGA_OK;
+}
+
+int gpuga_server_hold(gpuga_server* s, int on) {
+  if (!s) {
+    set_error("gpuga_server_hold: null server");
+    return GPUGA_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> g(s->mu);
+  s->hold = on != 0;
+  s->cv.notify_all();
   return GPUGA_OK;
 }
 
@@ -444,9 +586,11 @@ int gpuga_server_drain(gpuga_server* s, double timeout_s) {
   std::unique_lock<std::mutex> lock(s->mu);
   const auto deadline = Clock::now() + std::chrono::duration_cast<Clock::duration>(
                                            std::chrono::duration<double>(timeout_s > 0 ? timeout_s : 1e9));
-  while (!(s->queue.empty() && s->running.empty()) && s->worker_status == GPUGA_OK) {
-    if (s->idle_cv.wait_until(lock, deadline) == std::cv_status::timeout &&
-        !(s->queue.empty() && s->running.empty())) {
+  auto idle = [&] {
+    return s->queue.empty() && s->loading == 0 && s->ready.empty() && s->running.empty() && s->retiring.empty();
+  };
+  while (!idle() && s->worker_status == GPUGA_OK) {
+    if (s->idle_cv.wait_until(lock, deadline) == std::cv_status::timeout && !idle()) {
       set_error("gpuga_server_drain: jobs still running after %.1f s", timeout_s);
       return GPUGA_ERR_TIMEOUT;
     }
@@ -458,28 +602,25 @@ int gpuga_server_drain(gpuga_server* s, double timeout_s) {
   return GPUGA_OK;
 }
 
-int gpuga_server_stats(gpuga_server* s, double* out) {
-  if (!s || !out) {
-    set_error("gpuga_server_stats: null argument");
+int gpuga_server_stats(gpuga_server* s, double* out, int n) {
+  if (!s || !out || n < 0) {
+    set_error("gpuga_server_stats: invalid argument");
     return GPUGA_ERR_ARG;
   }
   std::lock_guard<std::mutex> g(s->mu);
-  std::vector<double> t = s->tick_ms;
-  std::sort(t.begin(), t.end());
-  auto pct = [&](double q) {
-    if (t.empty()) return 0.0;
-    const double pos = q * (t.size() - 1);
-    const size_t lo = (size_t)std::floor(pos), hi = (size_t)std::ceil(pos);
-    return t[lo] + (t[hi] - t[lo]) * (pos - lo);
-  };
-  out[0] = (double)s->batches;
-  out[1] = (double)s->finished;
-  out[2] = pct(0.50);
-  out[3] = pct(0.99);
-  out[4] = s->busy_s > 0 ? s->evals / s->busy_s : 0.0;
-  out[5] = (double)s->bytes_in_use;
-  out[6] = (double)s->peak_resident;
-  out[7] = s->evals;
+  const double v[] = {(double)s->batches,
+                      (double)s->finished,
+                      percentile(s->tick_ms, 0.50),
+                      percentile(s->tick_ms, 0.99),
+                      s->busy_s > 0 ? s->evals / s->busy_s : 0.0,
+                      (double)s->bytes_in_use,
+                      (double)s->peak_resident,
+                      s->evals,
+                      percentile(s->wall_ms, 0.50),
+                      percentile(s->wall_ms, 0.99),
+                      s->busy_s};
+  const int m = std::min(n, (int)(sizeof(v) / sizeof(v[0])));
+  for (int k = 0; k < m; ++k) out[k] = v[k];
   return GPUGA_OK;
 }
 
@@ -488,11 +629,19 @@ int gpuga_server_destroy(gpuga_server* s) {
   {
     std::lock_guard<std::mutex> g(s->mu);
     s->stop = true;
+    s->hold = false;
     for (Job* j : s->queue) j->cancel_requested = true;
     for (Job* j : s->running) j->cancel_requested = true;
+    for (Job* j : s->ready) j->cancel_requested = true;
     s->cv.notify_all();
+    s->loader_cv.notify_all();
   }
   if (s->worker.joinable()) s->worker.join();
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    s->loader_cv.notify_all();
+  }
+  if (s->loader.joinable()) s->loader.join();
   for (auto& kv : s->jobs)
     if (kv.second->engine && !kv.second->shared) delete kv.second->engine;
   delete s;

@@ -193,14 +193,18 @@ class Server:
     def cancel(self, job_id: int) -> None:
         check(_lib.load().gpuga_server_cancel(self._h, job_id))
 
+    def hold(self, on: bool = True) -> None:
+        """While held no new scheduling window starts; jobs are still admitted and set up."""
+        check(_lib.load().gpuga_server_hold(self._h, int(on)))
+
     def drain(self, timeout_s: float = 0.0) -> int:
         return _lib.load().gpuga_server_drain(self._h, float(timeout_s))
 
     def stats(self) -> dict:
-        s = np.zeros(8)
-        check(_lib.load().gpuga_server_stats(self._h, _p(s)))
         keys = ("batches", "jobs_finished", "p50_gen_ms", "p99_gen_ms", "evals_per_s", "device_bytes",
-                "peak_resident_jobs", "total_evals")
+                "peak_resident_jobs", "total_evals", "p50_wall_gen_ms", "p99_wall_gen_ms", "busy_s")
+        s = np.zeros(len(keys))
+        check(_lib.load().gpuga_server_stats(self._h, _p(s), len(keys)))
         return dict(zip(keys, (float(v) for v in s)))
 
     def close(self):

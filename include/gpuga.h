@@ -214,11 +214,14 @@ int gpuga_potential_destroy(gpuga_potential* p);
  * _find_force in one call that allocates nothing, for callers that cannot call cudaMalloc when
  * they need forces (a code that gives its whole device-memory budget to its own allocator, a
  * plug-in host that forbids device allocation after initialisation).  The caller passes all
- * inputs and outputs (device pointers, reference layouts); the scratch is a fixed 64 MiB array
- * per device inside the library, so N * max_Na * 56 bytes (+ the NN2B weights) must fit in it,
+ * inputs and outputs: `params` is a HOST array of num_params floats (decoded parameters in
+ * potential.in order, read during the call; NN2B weights are copied from it), every other
+ * pointer is a device pointer in the reference layouts.  The scratch is a fixed 64 MiB array per
+ * device inside the library, so N * max_Na * 56 bytes (+ the NN2B weights) must fit in it,
  * otherwise GPUGA_ERR_ARG.  The first call on a device looks up that array's address and should
- * come before any stream capture.  All calls on a device share the array: calls whose GPU work
- * overlaps race on it, so serialise them. */
+ * come before any stream capture; the address is kept for the life of the process, so do not
+ * call this entry point on a device after cudaDeviceReset.  All calls on a device share the
+ * array: calls whose GPU work overlaps race on it, so serialise them. */
 int gpuga_potential_find_force_noalloc(int potential_type, int num_neurons, const float* params, int num_params,
                                        int Nc, int N, const int* Na, const int* Na_sum, int max_Na, const int* type,
                                        const float* h, const int* NN, const int* NL, const float* r, float* f,
@@ -247,12 +250,16 @@ int gpuga_server_poll(gpuga_server* s, int job_id, int* progress_out);
 /* Best fitness history and final elite of a finished job: best_out float[generations], elite01_out float[num_vars] */
 int gpuga_server_result(gpuga_server* s, int job_id, float* best_out, float* elite01_out);
 int gpuga_server_cancel(gpuga_server* s, int job_id);
+/* on != 0: no new scheduling window starts (the one in flight finishes); jobs keep being admitted
+ * and set up, and start together once the hold is released (on = 0). */
+int gpuga_server_hold(gpuga_server* s, int on);
 /* Runs the scheduler until every submitted job is finished (or timeout_s elapses, -> GPUGA_ERR_TIMEOUT). */
 int gpuga_server_drain(gpuga_server* s, double timeout_s);
-/* stats: {generation batches run, jobs finished, p50 and p99 of the device time of a generation of all
- *         resident jobs (ms), aggregate evals/s over the windows' wall time, device bytes in use,
- *         peak jobs resident, total evals} */
-int gpuga_server_stats(gpuga_server* s, double* stats8);
+/* Fills stats[0 .. n-1] (n <= 11) with: {generation batches run, jobs finished, p50 and p99 of the
+ *         device time of a generation of all resident jobs (ms), aggregate evals/s over the busy wall
+ *         time, device bytes in use, peak jobs resident, total evals, p50 and p99 of the wall-clock time
+ *         per generation as each job saw it (ms; every stall included), busy wall time (s)} */
+int gpuga_server_stats(gpuga_server* s, double* stats, int n);
 int gpuga_server_destroy(gpuga_server* s);
 
 #ifdef __cplusplus

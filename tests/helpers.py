@@ -45,3 +45,31 @@ def synthetic_dir(oracle_mod, config: int, Nc: int, tmpdir: str, seed=None) -> t
     data = synth.make(config, seed=seed, Nc=Nc)
     data = synth.fill_targets(data, oracle_targets(oracle_mod))
     return synth.write_dir(data, tmpdir), data
+
+
+def golden_subset(src: str, dst: str, n_force: int, n_ev: int) -> str:
+    """A smaller copy of a training set: its first n_force force configurations and first n_ev
+    energy/virial configurations, train.in in the reference format (fitness.cu:95-148), the other
+    input files unchanged."""
+    import shutil
+    os.makedirs(dst, exist_ok=True)
+    for fn in os.listdir(src):
+        if fn != "train.in":
+            shutil.copy(os.path.join(src, fn), os.path.join(dst, fn))
+    with open(os.path.join(src, "train.in")) as f:
+        lines = [ln for ln in f.read().splitlines() if ln.strip()]
+    Nc, Ncf = (int(v) for v in lines[0].split()[:2])
+    Na = [int(lines[1 + c].split()[0]) for c in range(Nc)]
+    blocks, pos = [], 1 + Nc
+    for c in range(Nc):
+        n = Na[c] + 1 + (1 if c >= Ncf else 0)
+        blocks.append(lines[pos:pos + n])
+        pos += n
+    keep = list(range(min(n_force, Ncf))) + list(range(Ncf, min(Ncf + n_ev, Nc)))
+    kf = min(n_force, Ncf)
+    out = [f"{len(keep)} {kf}"] + [str(Na[c]) for c in keep]
+    for c in keep:
+        out += blocks[c]
+    with open(os.path.join(dst, "train.in"), "w") as f:
+        f.write("\n".join(out) + "\n")
+    return dst

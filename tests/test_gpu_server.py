@@ -50,13 +50,19 @@ def _pop_size(d):
 def test_jobs_are_the_same_alone_and_in_the_mix(job_dirs):
     refs = [alone(d, 1000 + k) for k, d in enumerate(job_dirs)]
     with Server(device=0, hbm_budget_bytes=120e9, max_jobs=32) as srv:
+        srv.hold(True)  # load every job first, so that all four share every window
         ids = [srv.submit(d, seed=1000 + k, generations=GENS) for k, d in enumerate(job_dirs)]
+        deadline = time.time() + 120
+        while any(srv.poll(j)[3] == Server.QUEUED for j in ids) and time.time() < deadline:
+            time.sleep(0.01)
+        srv.hold(False)
         assert srv.drain(300) == _lib.OK
         st = srv.stats()
         assert st["jobs_finished"] == len(job_dirs)
         assert st["peak_resident_jobs"] == len(job_dirs)  # all four shared the launches
         assert st["batches"] == GENS
         assert st["p99_gen_ms"] >= st["p50_gen_ms"] > 0
+        assert st["p99_wall_gen_ms"] >= st["p50_wall_gen_ms"] > 0
         for jid, d, (best, elite) in zip(ids, job_dirs, refs):
             status, done, total, state = srv.poll(jid)
             assert (status, done, total, state) == (_lib.OK, GENS, GENS, Server.DONE)

@@ -17,7 +17,7 @@ import pytest
 import torch
 
 from gpuga_b200 import _lib
-from tests.helpers import read_elite
+from tests.helpers import golden_subset, read_elite
 
 pytestmark = pytest.mark.gpu
 
@@ -39,18 +39,43 @@ def _within(got, want):
     return np.abs(g - w).max() <= RTOL_OF_SCALE * scale
 
 
-@pytest.mark.parametrize("name", ["si_diamond", "nn2b"])
-def test_noalloc_matches_allocating_entry_point(name, golden, built_oracle):
+def _synthetic(name, tmp_path):
+    """A small rigid-ion set (4 configurations of the rigid-ion benchmark geometry) and a Tersoff set
+    whose scratch, N * max_Na * 56 bytes, sits just under the fixed 64 MiB (2328 atoms x 512)."""
+    from gpuga_b200 import synth
+    if name == "synth_ri":
+        data = synth.make(3, Nc=4)
+    else:
+        data = synth.diamond_set([4, 4, 4, 4, 3, 2], Nc_force=3)
+    d = synth.write_dir(data, str(tmp_path / name))
+    return d, synth.teacher_params(data)
+
+
+# golden sets beyond the fixed scratch are cut to a few configurations (force, energy/virial)
+SUBSETS = {"wurzite_GaAs": (4, 8), "hfo2": (1, 1)}
+
+
+@pytest.mark.parametrize("name", ["si_diamond", "wurzite_GaAs", "hfo2", "nn2b", "synth_ri", "near_limit"])
+def test_noalloc_matches_allocating_entry_point(name, golden, built_oracle, tmp_path):
     L = _lib.load()
-    d = golden(name)
+    if name.startswith("synth") or name == "near_limit":
+        d, params = _synthetic(name, tmp_path)
+    else:
+        d = golden(name)
+        if name in SUBSETS:
+            d = golden_subset(d, str(tmp_path / name), *SUBSETS[name])
+        params = read_elite(d)
     s = built_oracle.OracleSet(d)
+    if name == "near_limit":
+        need = s.N * s.max_Na * 56
+        assert 0.95 * (64 << 20) < need < (64 << 20)
     a = {k: _dev(v) for k, v in s.arrays().items()}
     N, M, Nc = s.N, s.max_Na, s.Nc
     NN = torch.zeros(N, dtype=torch.int32, device="cuda")
     NL = torch.zeros(M * N, dtype=torch.int32, device="cuda")
     _lib.check(L.gpuga_neighbor_compute(Nc, N, M, _ptr(a["Na"]), _ptr(a["Na_sum"]), _ptr(a["r"]), _ptr(a["h"]),
                                         C.c_float(s.cutoff), _ptr(NN), _ptr(NL), None))
-    params = read_elite(d).astype(np.float32)
+    params = np.ascontiguousarray(params, dtype=np.float32)
     pp = params.ctypes.data_as(C.c_void_p)
 
     def outputs():
