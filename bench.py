@@ -70,19 +70,28 @@ def parse_args():
 
 # ----------------------------------------------------------------------------- plumbing
 class Dist:
-    def __init__(self):
+    """One process per GPU (torchrun environment): the barrier and the max-over-ranks timer.
+    backend: "nccl" on GPUs (the default when CUDA is available), "gloo" for the CPU tests."""
+
+    def __init__(self, backend: str | None = None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.device = "cpu"
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local_rank)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                    device_id=torch.device("cuda", self.local_rank))
+            backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+            timeout = datetime.timedelta(seconds=300)
+            if backend == "nccl":
+                torch.cuda.set_device(self.local_rank)
+                self.device = f"cuda:{self.local_rank}"
+                dist.init_process_group("nccl", timeout=timeout, device_id=torch.device("cuda", self.local_rank))
+            else:
+                dist.init_process_group(backend, timeout=timeout)
             self.pg = dist
 
     def barrier(self):
@@ -93,13 +102,21 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
+
+
+def whole_job_rate(dist: Dist, units_per_rank_step: float, step_ms) -> tuple:
+    """Whole-job throughput of K timed steps: every rank processed units_per_rank_step per step
+    (weak scaling), the job took the slowest rank's total device time.  Returns (units/s,
+    ms per step of the slowest rank)."""
+    total_ms = dist.max(float(sum(step_ms)))
+    return dist.world * units_per_rank_step * len(step_ms) / (total_ms / 1e3), total_ms / len(step_ms)
 
 
 class ClockSampler:
@@ -271,9 +288,7 @@ def run_ours(args, dist: Dist):
     torch.cuda.synchronize()
     clock_info = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = dist.max(sum(step_ms))
-    ms_per_step = total_ms / nsteps
-    value = dist.world * P * Natoms * nsteps / (total_ms / 1e3)
+    value, ms_per_step = whole_job_rate(dist, P * Natoms, step_ms)
     fit_dev = fit.cpu().numpy().copy()
 
     # ---- per-launch device times (separate pass of K steps; the launches of a step run one after

@@ -303,7 +303,8 @@ using Geo = GeoT<-1>;
 // slots, with all threads of the CTA (independent loads, then one barrier).
 // D64: the FP64 bond lengths (FP64 pair terms), else their FP32 remainders.
 template <int ZC, bool D64>
-__device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int Na, bool force, unsigned char* base) {
+__device__ __forceinline__ Geo stage_geometry(const DevView& S, int c, int atom0, int Na, bool force,
+                                              unsigned char* base) {
   const int n = ZC * Na;
   float4* sg = reinterpret_cast<float4*>(base);
   double* sd = reinterpret_cast<double*>(sg + n);
@@ -311,15 +312,26 @@ __device__ __forceinline__ Geo stage_geometry(const DevView& S, int atom0, int N
   int* snn = reinterpret_cast<int*>(sl + (D64 ? 0 : n));
   int* srev = snn + Na;
   uint8_t* spt = reinterpret_cast<uint8_t*>(srev + (force ? n : 0));
-  for (int t = threadIdx.x; t < n; t += blockDim.x) {
-    const int j = t / Na, il = t - j * Na, i = atom0 + il;
-    if (j < S.NN[i]) {
-      const int b = S.off[i] + j;
-      sg[t] = __ldg(&S.g32[b]);
-      if (D64) sd[t] = __ldg(&S.d64[b]);
-      else sl[t] = __ldg(&S.tdl[b]);
-      spt[t] = S.ptype[b];
-      if (force) srev[t] = S.rev_sm[b];
+  if (!D64 && S.g_sm) {
+    // a straight copy of the slot-major global layout
+    const int o = S.sm_off[c];
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      sg[t] = __ldg(&S.g_sm[o + t]);
+      sl[t] = __ldg(&S.dl_sm[o + t]);
+      spt[t] = S.pt_sm[o + t];
+      if (force) srev[t] = S.rev_sm_sm[o + t];
+    }
+  } else {
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      const int j = t / Na, il = t - j * Na, i = atom0 + il;
+      if (j < S.NN[i]) {
+        const int b = S.off[i] + j;
+        sg[t] = __ldg(&S.g32[b]);
+        if (D64) sd[t] = __ldg(&S.d64[b]);
+        else sl[t] = __ldg(&S.tdl[b]);
+        spt[t] = S.ptype[b];
+        if (force) srev[t] = S.rev_sm[b];
+      }
     }
   }
   for (int k = threadIdx.x; k < Na; k += blockDim.x) snn[k] = S.NN[atom0 + k];
@@ -353,6 +365,7 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
   const int Z = FULL ? ZC : geo.nn[il];
   const int b0 = geo.base(il), bs = geo.step();  // bond j at b0 + j * bs
   float ux[ZC], uy[ZC], uz[ZC], dd[ZC];
+  double d64[PM == kPair64 ? ZC : 1];  // FP64 lengths, loaded with the rest of the geometry
   int st[ZC];
 #pragma unroll
   for (int j = 0; j < ZC; ++j) {
@@ -363,10 +376,12 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
       uy[j] = q.y;
       uz[j] = q.z;
       dd[j] = q.w;
+      if constexpr (PM == kPair64) d64[j] = geo.d64[b0 + j * bs];
       if (NT == 2) st[j] = geo.pt[b0 + j * bs];
     } else {
       ux[j] = uy[j] = uz[j] = 0.f;
       dd[j] = 1.0f;
+      if constexpr (PM == kPair64) d64[j] = 1.0;
     }
   }
   // pass A: cutoff of every bond
@@ -420,21 +435,30 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
       const int s = NT == 2 ? st[j] : 0;
       float fa32;
       if constexpr (PM == kPair64) {
-        const double t = geo.d64[b0 + j * bs] - (s ? C.r064[1] : C.r064[0]);
+        // exponentials to 7e-12 (exp_d.cuh), far below the FP32 rounding of A'_j
+        const double t = d64[j] - (s ? C.r064[1] : C.r064[0]);
         const double la = s ? C.la64[1] : C.la64[0];
-        const double ea = exp_d<10>(-la * t);
+        const double ea = exp_d_clamped<9>(-la * t);
         const double fa = (s ? C.ca64[1] : C.ca64[0]) * ea;
-        const double fr = LO ? (s ? C.cr64[1] : C.cr64[0]) * exp_d<10>(-(s ? C.lr64[1] : C.lr64[0]) * t)
-                             : 0.5 * fa * ea;
-        const double lr_fr = LO ? (s ? C.lr64[1] : C.lr64[0]) * fr : 2.0 * la * fr;
         const double bd = b;
-        const double e = fr - bd * fa;
+        double e, dA;  // fr - b fa and fr' - b fa'
+        if constexpr (LO) {
+          const double lr = s ? C.lr64[1] : C.lr64[0];
+          const double fr = (s ? C.cr64[1] : C.cr64[0]) * exp_d_clamped<9>(-lr * t);
+          e = fma(-bd, fa, fr);
+          dA = fma(bd * la, fa, -lr * fr);
+        } else {
+          // S = 2: fr = fa e / 2 and fr' - b fa' = la (b fa - 2 fr) = -la (e + fr)
+          const double fr = 0.5 * fa * ea;
+          e = fma(-bd, fa, fr);
+          dA = -la * (e + fr);
+        }
         if (fc[j] == 1.0f && fcp[j] == 0.0f) {  // inside r1: no conversions of fc, fc'
           pe = fma(0.5, e, pe);
-          Ap[j] = (float)fma(bd * la, fa, -lr_fr);
+          Ap[j] = (float)dA;
         } else {
           pe = fma(0.5 * (double)fc[j], e, pe);
-          Ap[j] = (float)fma((double)fcp[j], e, (double)fc[j] * fma(bd * la, fa, -lr_fr));
+          Ap[j] = (float)fma((double)fcp[j], e, (double)fc[j] * dA);
         }
         fa32 = (float)fa;
       } else {
@@ -556,9 +580,14 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
     for (int k = 0; k < 7; ++k) red[k * BLK + threadIdx.x] = 0.0;
   }
   GeoT<ST> geo;
-  if (ST == 1 || (ST == -1 && item_staged(it))) {
-    const Geo s0 = stage_geometry<ZC, PM == kPair64>(S, atom0, Na, FORCE, smem + front);
+  if ((ST == 1 || ST == -1) && item_staged(it)) {
+    const Geo s0 = stage_geometry<ZC, PM == kPair64>(S, c, atom0, Na, FORCE, smem + front);
     geo = GeoT<ST>{s0.g, s0.d64, s0.dlo, s0.pt, s0.rev, s0.nn, s0.boff, s0.bond0, s0.stride};
+  } else if (FORCE && ST != 0) {
+    // force items read the slot-major global copy: the lanes of a warp hold consecutive atoms and
+    // read consecutive words, as from the staged copy
+    const int o = S.sm_off[c];
+    geo = GeoT<ST>{S.g_sm + o, nullptr, S.dl_sm + o, S.pt_sm + o, S.rev_sm_sm + o, S.NN + atom0, nullptr, 0, Na};
   } else {
     geo = GeoT<ST>{S.g32 + bond0, S.d64 + bond0, S.tdl + bond0, S.ptype + bond0, S.rev_sm + bond0, S.NN + atom0,
                    S.off + atom0, bond0, 0};
@@ -637,11 +666,9 @@ __global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_ba
     // specialisation spilled at this kernel's register bound and ran 5 % slower)
     tersoff_item<ZC, NT, FORCE, BLK, 32, -1, LO>(jobs, it, smem);
   } else if constexpr (ZC == 4) {
-    const bool st = item_staged(it);
-#define GPUGA_TI(GG)                                                     \
-  case GG:                                                               \
-    if (st) tersoff_item<ZC, NT, FORCE, BLK, GG, 1, LO>(jobs, it, smem);     \
-    else tersoff_item<ZC, NT, FORCE, BLK, GG, 0, LO>(jobs, it, smem);        \
+#define GPUGA_TI(GG)                                    \
+  case GG:                                              \
+    tersoff_item<ZC, NT, FORCE, BLK, GG, 1, LO>(jobs, it, smem); \
     break;
     switch (item_G(it)) {
       GPUGA_TI(32)
@@ -1153,7 +1180,7 @@ size_t stage_target(int zc) { return zc == 4 ? 74 * 1024 : 110 * 1024; }  // for
 constexpr int kBlockEV = 128;
 constexpr size_t kSmemMax = 220 * 1024;
 
-int zclass_of(int z) { return z <= 4 ? 4 : (z <= 8 ? 8 : (z <= 16 ? 16 : 0)); }
+int zclass_of(int z) { return tersoff_zclass(z); }
 int nmax_of(int n) { return n <= 8 ? 8 : (n <= 16 ? 16 : (n <= 32 ? 32 : 0)); }
 }  // namespace
 
@@ -1172,6 +1199,11 @@ DevView make_view(const DevSet& d) {
   v.g32 = d.g32;
   v.d64 = d.d64;
   v.tdl = d.tdl;
+  v.sm_off = d.sm_off;
+  v.g_sm = d.g_sm;
+  v.dl_sm = d.dl_sm;
+  v.pt_sm = d.pt_sm;
+  v.rev_sm_sm = d.rev_sm_sm;
   v.rg32 = d.rg32;
   v.rdl = d.rdl;
   v.rseg = d.rseg;

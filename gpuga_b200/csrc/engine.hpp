@@ -36,6 +36,10 @@ constexpr int kMaxConsts = 32;        // per-individual FP32 constants of the ba
 constexpr int kRiAtomLin = 27;        // RI linear force sums per force atom: 3 pair types x 3 x xyz
 constexpr int kRiCfgLin = 66;         // RI linear energy/virial sums per configuration: 3 x (4 + 3 x 6)
 
+// Register-array size of the batched Tersoff kernels for a configuration whose atoms have at most
+// z neighbors (0: beyond the supported 16).
+inline int tersoff_zclass(int z) { return z <= 4 ? 4 : (z <= 8 ? 8 : (z <= 16 ? 16 : 0)); }
+
 struct DevSet {
   int Nc = 0, Nc_force = 0, N = 0, N_force = 0, B = 0, max_Na = 0, max_Z = 0;
   int potential_type = -1, num_types = 1, num_neurons = 0, num_vars = 0;
@@ -55,6 +59,14 @@ struct DevSet {
   double4* g64 = nullptr;
   double* d64 = nullptr;   // Tersoff: FP64 bond lengths (the FP64 pair terms)
   float* tdl = nullptr;    // Tersoff: d - (float)d (the FP32 pair terms' correction)
+  // Tersoff: a slot-major copy of the bond geometry, per configuration c at sm_off[c] with
+  // tersoff_zclass(max Z of c) slots: bond j of local atom il at sm_off[c] + j * Na + il (the
+  // layout of the force kernels' staged geometry and f_ij scratch; empty slots zero)
+  int* sm_off = nullptr;
+  float4* g_sm = nullptr;
+  float* dl_sm = nullptr;
+  uint8_t* pt_sm = nullptr;
+  int* rev_sm_sm = nullptr;
   // RI batched lists: per atom the pairs its work items evaluate pair by pair (the full list
   // for force configurations, the half list for energy/virial ones; only pair types whose
   // Buckingham or Morse term can be nonzero, ri_active) grouped by pair type, in list order
@@ -102,6 +114,11 @@ struct DevView {
   const float4* g32;
   const double* d64;
   const float* tdl;
+  const int* sm_off;
+  const float4* g_sm;
+  const float* dl_sm;
+  const uint8_t* pt_sm;
+  const int* rev_sm_sm;
   const float4* rg32;
   const float* rdl;
   const int4* rseg;

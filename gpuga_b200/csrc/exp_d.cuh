@@ -76,4 +76,29 @@ GPUGA_EXPD_HD double exp_d(double x) {
   return x < -708.0 ? 0.0 : (x > 708.0 ? INFINITY : y);
 }
 
+// The same exponential for arguments the caller knows to be finite: x is clamped to
+// [-708, 708] (e^-708 ~ 3e-308 and e^708 ~ 3e307 stand in for 0 and +inf beyond) and a NaN
+// argument propagates through the final addition of x - x; no comparisons or selects.
+template <int DEG = 13>
+GPUGA_EXPD_HD double exp_d_clamped(double x) {
+  static_assert(DEG >= 8 && DEG <= 13, "exp_d_clamped: Taylor degree 8..13");
+  const double log2e = 0x1.71547652b82fep+0;
+  const double ln2_hi = 0x1.62e42ff000000p-1;
+  const double ln2_lo = -0x1.718432a1b0e26p-35;
+  const double shifter = 0x1.8p52;
+  const double xc = fmin(fmax(x, -708.0), 708.0);
+  const double kd_s = fma(xc, log2e, shifter);
+  const int64_t k = (int64_t)(int32_t)(uint32_t)expd_bits(kd_s);
+  const double kd = kd_s - shifter;
+  double r = fma(-kd, ln2_hi, xc);
+  r = fma(-kd, ln2_lo, r);
+  constexpr double inv_fact[14] = {1.0,        1.0,         0.5,          1.0 / 6.0,     1.0 / 24.0,
+                                   1.0 / 120.0, 1.0 / 720.0, 1.0 / 5040.0, 1.0 / 40320.0, 1.0 / 362880.0,
+                                   1.0 / 3628800.0, 1.0 / 39916800.0, 1.0 / 479001600.0, 1.0 / 6227020800.0};
+  double p = inv_fact[DEG];
+#pragma unroll
+  for (int i = DEG - 1; i >= 0; --i) p = fma(p, r, inv_fact[i]);
+  return expd_from_bits(expd_bits(p) + (k << 52)) + (x - x);
+}
+
 }  // namespace gpuga

@@ -476,6 +476,75 @@ void build_cell_lists(const Engine* e, CellLists* cl) {
   }
 }
 
+// Tersoff: bond j of local atom il of configuration c copied to sm_off[c] + j * Na + il (empty
+// slots zero), one thread per atom.
+__global__ void slot_major_copy(int N, const int* __restrict__ atom_cfg, const int* __restrict__ Na_sum,
+                                const int* __restrict__ Na, const int* __restrict__ sm_off,
+                                const int* __restrict__ zc_of, const int* __restrict__ off,
+                                const float4* __restrict__ g32, const float* __restrict__ tdl,
+                                const uint8_t* __restrict__ ptype, const int* __restrict__ rev_sm,
+                                float4* __restrict__ g_sm, float* __restrict__ dl_sm, uint8_t* __restrict__ pt_sm,
+                                int* __restrict__ rev_sm_sm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int c = atom_cfg[i], il = i - Na_sum[c], na = Na[c];
+  const int Z = off[i + 1] - off[i];
+  for (int j = 0; j < zc_of[c]; ++j) {
+    const size_t o = (size_t)sm_off[c] + (size_t)j * na + il;
+    if (j < Z) {
+      const int b = off[i] + j;
+      g_sm[o] = g32[b];
+      dl_sm[o] = tdl[b];
+      pt_sm[o] = ptype[b];
+      rev_sm_sm[o] = rev_sm[b];
+    } else {
+      g_sm[o] = make_float4(0.f, 0.f, 0.f, 1.f);
+      dl_sm[o] = 0.f;
+      pt_sm[o] = 0;
+      rev_sm_sm[o] = 0;
+    }
+  }
+}
+
+// The slot-major copy of the Tersoff geometry (DevSet::g_sm and friends).
+static int build_slot_major(Engine* e, cudaStream_t st) {
+  DevSet& d = e->d;
+  const TrainingSet& ts = e->ts;
+  const int Nc = ts.Nc, N = ts.N;
+  std::vector<int> offs(Nc), zcs(Nc), atom_cfg(N);
+  long long total = 0;
+  for (int c = 0; c < Nc; ++c) {
+    zcs[c] = std::max(tersoff_zclass(e->h_zmax[c]), 1);  // beyond 16 neighbors: refused at planning
+    if (zcs[c] == 1) zcs[c] = 16;
+    offs[c] = (int)total;
+    total += (long long)zcs[c] * ts.Na[c];
+    for (int k = 0; k < ts.Na[c]; ++k) atom_cfg[ts.Na_sum[c] + k] = c;
+  }
+  if (total > (1LL << 31) - 1) {
+    set_error("slot-major geometry of %lld slots exceeds int32 indexing.", total);
+    return GPUGA_ERR_UNSUPPORTED;
+  }
+  const size_t n = std::max<long long>(total, 1);
+  GPUGA_TRY(e->alloc(&d.sm_off, std::max(Nc, 1)));
+  GPUGA_TRY(e->alloc(&d.g_sm, n));
+  GPUGA_TRY(e->alloc(&d.dl_sm, n));
+  GPUGA_TRY(e->alloc(&d.pt_sm, n));
+  GPUGA_TRY(e->alloc(&d.rev_sm_sm, n));
+  int *d_zc = nullptr, *d_cfg = nullptr;
+  GPUGA_CUDA(cudaMalloc(&d_zc, sizeof(int) * std::max(Nc, 1)));
+  GPUGA_CUDA(cudaMalloc(&d_cfg, sizeof(int) * std::max(N, 1)));
+  GPUGA_CUDA(cudaMemcpyAsync(d.sm_off, offs.data(), sizeof(int) * Nc, cudaMemcpyHostToDevice, st));
+  GPUGA_CUDA(cudaMemcpyAsync(d_zc, zcs.data(), sizeof(int) * Nc, cudaMemcpyHostToDevice, st));
+  GPUGA_CUDA(cudaMemcpyAsync(d_cfg, atom_cfg.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
+  slot_major_copy<<<(N + 127) / 128, 128, 0, st>>>(N, d_cfg, d.Na_sum, d.Na, d.sm_off, d_zc, d.off, d.g32, d.tdl,
+                                                   d.ptype, d.rev_sm, d.g_sm, d.dl_sm, d.pt_sm, d.rev_sm_sm);
+  GPUGA_CUDA(cudaGetLastError());
+  GPUGA_CUDA(cudaStreamSynchronize(st));
+  cudaFree(d_zc);
+  cudaFree(d_cfg);
+  return GPUGA_OK;
+}
+
 // Pair types whose Buckingham or Morse term can be nonzero for some individual: type t is left
 // out of the pair-by-pair lists when its bounds fix A_t = 0 with rho_t > 0 (A e^{-d/rho} is then
 // exactly zero) and, for the cation-anion type, the Morse D0 is fixed at 0 as well.
@@ -661,6 +730,7 @@ int build_geometry(Engine* e) {
   e->h_zmax.assign(Nc, 0);
   for (int c = 0; c < Nc; ++c)
     for (int k = 0; k < ts.Na[c]; ++k) e->h_zmax[c] = std::max(e->h_zmax[c], e->h_NN[ts.Na_sum[c] + k]);
+  if (tersoff) GPUGA_TRY(build_slot_major(e, st));
   return GPUGA_OK;
 }
 

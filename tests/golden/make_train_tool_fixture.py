@@ -7,7 +7,7 @@ configurations, the last 3 from other_poly/ as in the reference's input.txt)
 and stores, under tests/golden/train_tool/<set>/, the input files, input.txt
 and the train.in the reference program wrote.
 
-    python tests/golden/make_train_tool_fixture.py
+    python tests/golden/make_train_tool_fixture.py [path/to/reference]
 """
 import os
 import shutil
@@ -16,7 +16,10 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference/develop/wurzite"
+import sys
+
+REFERENCE = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GPUGA_REFERENCE", "/root/reference")
+REF = os.path.join(REFERENCE, "develop", "wurzite")
 
 FILES = ["random/data_0", "random/data_1", "HIDROSTATIC/data_-0.010000", "BIAXIAL_0/data_-0.010000",
          "other_poly/data-bcc", "other_poly/data-rocksalt", "other_poly/data-zb"]

@@ -46,3 +46,27 @@ def test_sharded_population_equals_single_process(tmp_path, built_oracle):
     want = built_oracle.OracleSet(d).fitness(pop)
     np.testing.assert_array_equal(fit, want)
     assert float(np.load(tmp_path / "tmax.npy")[0]) == 2.0
+
+
+def _bench_worker(rank, world, port, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world), RANK=str(rank),
+                      LOCAL_RANK=str(rank))
+    import bench
+    d = bench.Dist(backend="gloo")
+    d.barrier()
+    # rank r timed its K = 4 steps at (r + 1) ms each: the job took the slowest rank's 8 ms
+    value, ms = bench.whole_job_rate(d, 1000.0, [float(rank + 1)] * 4)
+    if rank == 0:
+        np.save(os.path.join(out_dir, "rate.npy"), np.array([value, ms, d.world]))
+    d.barrier()
+    d.close()
+
+
+def test_bench_dist_aggregation(tmp_path):
+    """bench.py's multi-rank plumbing (the Dist barrier and max-over-ranks timer, the whole-job
+    rate) on two gloo ranks."""
+    mp.start_processes(_bench_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, start_method="spawn")
+    value, ms, world = np.load(tmp_path / "rate.npy")
+    assert world == 2
+    assert ms == 2.0                                 # slowest rank: 4 steps x 2 ms
+    assert value == 2 * 1000.0 * 4 / (8.0 / 1e3)     # both ranks' units over the slowest rank's time

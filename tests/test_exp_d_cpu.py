@@ -20,8 +20,10 @@ def test_exp_d_error_bound(tmp_path):
                     os.path.join(HERE, "exp_d_check.cpp")], check=True)
     out = subprocess.run([exe, "2000000"], capture_output=True, text=True, check=True).stdout.split()
     n, max_rel, mean_rel, bad, max10 = int(out[0]), float(out[1]), float(out[2]), int(out[3]), float(out[4])
+    max9c = float(out[5])
     assert n == 2000000
     assert max_rel <= 3e-16, max_rel      # measured 1.4e-16 (about one unit in the last place)
     assert mean_rel <= 1e-16, mean_rel    # measured 4e-17
     assert bad == 0
     assert max10 <= 4e-13, max10          # degree 10: truncation 2.3e-13
+    assert max9c <= 1.2e-11, max9c        # exp_d_clamped, degree 9: truncation 7.3e-12

@@ -58,7 +58,7 @@ def test_large_configuration_fitness_and_forces(large_set):
     with Fitness(arrays=data) as e:
         fit = e.compute(P, pop)
         fit64 = e.compute(P, pop, path=PATH_PLAIN64)
-        np.testing.assert_allclose(fit, fit64, rtol=2e-5)
+        np.testing.assert_allclose(fit, fit64, rtol=1e-6)
         assert np.array_equal(np.argsort(fit, kind="stable"), np.argsort(fit64, kind="stable"))
         # per-atom forces of the force configurations (4096-atom one through the global scratch)
         Fb = e.batched_forces(pop[:4])
@@ -69,4 +69,4 @@ def test_large_configuration_fitness_and_forces(large_set):
             scale = np.abs(want).max()
             np.testing.assert_allclose(Fb[k], want, atol=2e-5 * scale, rtol=0)
         # the oracle's FP64 fitness of the first individuals
-        np.testing.assert_allclose(fit[:4], s.fitness(pop[:4]), rtol=2e-5)
+        np.testing.assert_allclose(fit[:4], s.fitness(pop[:4]), rtol=1e-6)

@@ -2,7 +2,7 @@
 opt-in damped-Coulomb self energy (gpuga_options.ri_self_energy).
 
 Tolerances as in the main parity file: FP64 path 1e-9 of each quantity's scale; batched
-fitness relative 2e-5 per individual with the FP64 ranking; per-config energies 2e-6 of the
+fitness relative 1e-6 per individual with the FP64 ranking; per-config energies 2e-6 of the
 set's energy scale.  Type 0 with the self energy off is the reference's ri.cu and is covered
 there; here every other combination, plus the statement that switching the self energy on
 changes energies only."""
@@ -14,7 +14,7 @@ from tests.helpers import oracle_targets
 
 pytestmark = pytest.mark.gpu
 
-FIT_RTOL = 2e-5
+FIT_RTOL = 1e-6
 MODES = [(4, False), (0, True), (4, True)]
 
 
@@ -64,9 +64,7 @@ def test_batched_fitness_and_energies_match_oracle(ri_sets, pt, self_on):
         assert rel[1:].max() <= FIT_RTOL
         assert fit[0] < 1e-3 * np.median(fit[1:])  # the teacher reproduces the targets it made
         order, oorder = np.argsort(fit[1:], kind="stable"), np.argsort(ofit[1:], kind="stable")
-        if not np.array_equal(order, oorder):
-            srt = np.sort(ofit[1:])
-            assert (np.diff(srt) / np.abs(srt[1:])).min() <= 2 * FIT_RTOL
+        assert np.array_equal(order, oorder)
         E, _, _ = e.config_results(P)
         Ncf = s.Nc_force
         for p in (0, 1, P - 1):
