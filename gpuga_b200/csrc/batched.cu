@@ -543,6 +543,9 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
 // GT: the item's individuals per item G as a compile-time constant (0: read from the item), so
 // that the force scratch addressing and the atom-slot split fold into shifts and constants;
 // ST: staged (1) or in-place CSR (0) geometry, or decided per item (-1).
+// Bytes of the force items' shared-memory table of per-individual constants (G entries).
+__host__ __device__ constexpr size_t tersoff_table_bytes(int G) { return ((size_t)G * sizeof(TersoffC) + 15) & ~(size_t)15; }
+
 // Pair-term form of the two kinds of Tersoff items (tersoff_atom, PairMode).  Energy/virial items
 // take the FP64 pair terms: the configuration virial sums the radial forces of all bonds, whose
 // cancellation near equilibrium amplifies FP32 rounding.  Force items stay FP32: their force error
@@ -566,15 +569,23 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
   const int g = lane & (G - 1), aslot = lane / G;
   const int p = it.p0 + g;
   const Consts kc{J.consts, J.Pstride, p < P ? p : it.p0};
-  TersoffC C;
-  load_tersoff<LO, PM>(kc, C);
+  TersoffC Creg;
+  load_tersoff<LO, PM>(kc, Creg);
   const int c = it.config, atom0 = S.Na_sum[c], Na = S.Na[c];
   const int bond0 = S.off[atom0];
+  // Force items keep the G individuals' constants in a shared-memory table at the start of the
+  // dynamic shared memory, read where used: the force kernel runs at its register bound, and
+  // constants held in registers across the atom loop were spilled to local memory.
+  const size_t tab = FORCE ? tersoff_table_bytes(G) : 0;
+  TersoffC* ctab = reinterpret_cast<TersoffC*>(smem);
+  if (FORCE && warp == 0 && aslot == 0) ctab[g] = Creg;
   // force scratch: shared memory, or for configurations too large for it the item's own
   // region of global memory (visible to the whole CTA after __syncthreads as well)
-  float* fsm = FORCE && item_global(it) ? J.gscratch + (size_t)it.gofs * 64 : reinterpret_cast<float*>(smem);
+  float* fsm = FORCE && item_global(it) ? J.gscratch + (size_t)it.gofs * 64 : reinterpret_cast<float*>(smem + tab);
   double* red = reinterpret_cast<double*>(smem);
-  const size_t front = FORCE ? item_fbytes(it) : (size_t)BLK * kResK * sizeof(double);
+  const size_t front = FORCE ? tab + item_fbytes(it) : (size_t)BLK * kResK * sizeof(double);
+  if (FORCE) __syncthreads();  // the constants table
+  const TersoffC& C = FORCE ? ctab[g] : Creg;
   if (!FORCE) {
 #pragma unroll
     for (int k = 0; k < 7; ++k) red[k * BLK + threadIdx.x] = 0.0;
@@ -1372,22 +1383,25 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
       const size_t stage =
           ((size_t)zc * Na * (16 + (d64 ? 8 : 4) + 1 + (force ? 4 : 0)) + (size_t)Na * 4 + 15) & ~(size_t)15;
       const size_t per_ind = (size_t)e->h_zmax[c] * Na * 3 * sizeof(float);  // slot-major, padded to max Z
-      if (force && per_ind > force_smem_target(zc)) {
+      // force items: the constants table (tersoff_table_bytes), the f_ij scratch, the staged geometry
+      auto scratch = [&](int g) { return tersoff_table_bytes(g) + ((per_ind * g + 15) & ~(size_t)15); };
+      if (force && scratch(1) > force_smem_target(zc)) {
         // not even one individual's scratch fits: 32 individuals per item (lane = individual,
         // coalesced scratch rows) with the scratch in global memory
         global = true;
         item_floats = ((per_ind / sizeof(float)) * 32 + 63) & ~(size_t)63;
+        smem = std::max(smem, kRedBytes + tersoff_table_bytes(32));
       } else if (force) {
-        while (G > 1 && per_ind * G > force_smem_target(zc)) G >>= 1;
+        while (G > 1 && scratch(G) > force_smem_target(zc)) G >>= 1;
         // stage the geometry too when it fits beside the scratch of >= 4 individuals
         int Gs = G;
-        while (Gs > 4 && ((per_ind * Gs + 15) & ~(size_t)15) + stage > stage_target(zc)) Gs >>= 1;
-        if (((per_ind * Gs + 15) & ~(size_t)15) + stage <= stage_target(zc)) {
+        while (Gs > 4 && scratch(Gs) + stage > stage_target(zc)) Gs >>= 1;
+        if (scratch(Gs) + stage <= stage_target(zc)) {
           G = Gs;
           staged = true;
         }
         fbytes = (per_ind * G + 15) & ~(size_t)15;
-        smem = std::max(smem, fbytes + (staged ? stage : 0));
+        smem = std::max(smem, scratch(G) + (staged ? stage : 0));
       } else {
         // energy/virial items (always G = 32, which tersoff_batched compiles in): per-lane FP64
         // sums of the 128-thread CTA, then (optionally) the geometry
