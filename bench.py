@@ -111,6 +111,21 @@ class Dist:
             self.pg.destroy_process_group()
 
 
+TILE_NAMES = {1: "fixed rule", 2: "half G", 3: "quarter G", 4: "32 per item, global scratch", 5: "unstaged"}
+
+
+def tile_summary(e, data, P) -> dict | None:
+    """The autotuner's force-item tile per force-configuration size (Tersoff sets)."""
+    if int(data["potential_type"]) not in (1, 2):
+        return None
+    codes, tune_ms = e.plan_tiles(P)
+    Na, Ncf = np.asarray(data["Na"]), int(data["Nc_force"])
+    by_size = {}
+    for c in range(Ncf):
+        by_size.setdefault(int(Na[c]), TILE_NAMES.get(int(codes[c]), str(int(codes[c]))))
+    return {"autotuned": True, "tune_ms": tune_ms, "force_tile_by_atoms": dict(sorted(by_size.items()))}
+
+
 def whole_job_rate(dist: Dist, units_per_rank_step: float, step_ms) -> tuple:
     """Whole-job throughput of K timed steps: every rank processed units_per_rank_step per step
     (weak scaling), the job took the slowest rank's total device time.  Returns (units/s,
@@ -267,6 +282,7 @@ def run_ours(args, dist: Dist):
 
     n_launch = C.c_int()
     _lib.check(L.gpuga_plan_info(h, P, C.byref(n_launch), None, 0))
+    tiles = tile_summary(e, data, P)
     kernels_per_step = n_launch.value + 2  # + decode + fitness fold
 
     # ---- value: device-resident inputs, device time per step, L2 flushed between steps
@@ -385,6 +401,7 @@ def run_ours(args, dist: Dist):
                        "max_rel_fitness_err_vs_fp64": float(rel.max()),
                        "p99_rel_fitness_err_vs_fp64": float(np.percentile(rel, 99)), "ranking_identical": rank_same},
         "ga_loop": ga_loop,
+        "tiles": tiles,
         "clocks": clock_info,
         "measured_peaks": {k: measured_peaks().get(k) for k in ("hbm_gbs", "bf16_tflops", "sm_max_mhz")},
         "fitness_checksum": float(np.sum(fit_dev)),

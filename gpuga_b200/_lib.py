@@ -32,7 +32,7 @@ class GpugaError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("device", C.c_int), ("path", C.c_int), ("use_graph", C.c_int), ("nn2b_consistent", C.c_int),
                 ("nn2b_r1", C.c_float), ("nn2b_r2", C.c_float), ("verbose", C.c_int), ("neighbor_cells", C.c_int),
-                ("ri_self_energy", C.c_int)]
+                ("ri_self_energy", C.c_int), ("tiles", C.c_int)]
 
 
 FITNESS_CB = C.CFUNCTYPE(None, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_void_p)
@@ -90,6 +90,7 @@ PROTOTYPES = {
     "gpuga_server_drain": (i32, [vp, C.c_double]),
     "gpuga_server_stats": (i32, [vp, vp, i32]),
     "gpuga_server_hold": (i32, [vp, i32]),
+    "gpuga_plan_tiles": (i32, [vp, i32, vp, i32, vp]),
     "gpuga_server_destroy": (i32, [vp]),
 }
 

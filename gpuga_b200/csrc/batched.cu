@@ -26,6 +26,7 @@
 // once (geometry.cu); three-body cosines are dot products of the FP32 unit
 // vectors, formed in registers.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <tuple>
 #include <type_traits>
@@ -545,6 +546,8 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
 // ST: staged (1) or in-place CSR (0) geometry, or decided per item (-1).
 // Bytes of the force items' shared-memory table of per-individual constants (G entries).
 __host__ __device__ constexpr size_t tersoff_table_bytes(int G) { return ((size_t)G * sizeof(TersoffC) + 15) & ~(size_t)15; }
+// Bytes of the force items' table of per-(individual, atom) squared force errors.
+__host__ __device__ constexpr size_t tersoff_ferr_bytes(int G, int Na) { return ((size_t)G * Na * sizeof(double) + 15) & ~(size_t)15; }
 
 // Pair-term form of the two kinds of Tersoff items (tersoff_atom, PairMode).  Energy/virial items
 // take the FP64 pair terms: the configuration virial sums the radial forces of all bonds, whose
@@ -580,10 +583,14 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
   TersoffC* ctab = reinterpret_cast<TersoffC*>(smem);
   if (FORCE && warp == 0 && aslot == 0) ctab[g] = Creg;
   // force scratch: shared memory, or for configurations too large for it the item's own
-  // region of global memory (visible to the whole CTA after __syncthreads as well)
-  float* fsm = FORCE && item_global(it) ? J.gscratch + (size_t)it.gofs * 64 : reinterpret_cast<float*>(smem + tab);
+  // region of global memory (visible to the whole CTA after __syncthreads as well); the
+  // per-(individual, atom) squared force errors ftab[g][il] before it (shared memory) or after
+  // it (global memory)
+  const bool glob = FORCE && item_global(it);
+  float* fsm = glob ? J.gscratch + (size_t)it.gofs * 64 : reinterpret_cast<float*>(smem + tab + tersoff_ferr_bytes(G, Na));
+  double* ftab = glob ? reinterpret_cast<double*>(fsm + (size_t)ZC * Na * 3 * 32) : reinterpret_cast<double*>(smem + tab);
   double* red = reinterpret_cast<double*>(smem);
-  const size_t front = FORCE ? tab + item_fbytes(it) : (size_t)BLK * kResK * sizeof(double);
+  const size_t front = FORCE ? tab + tersoff_ferr_bytes(G, Na) + item_fbytes(it) : (size_t)BLK * kResK * sizeof(double);
   if (FORCE) __syncthreads();  // the constants table
   const TersoffC& C = FORCE ? ctab[g] : Creg;
   if (!FORCE) {
@@ -624,7 +631,6 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
     return;
   }
   __syncthreads();
-  double ferr = 0.0;
   const int N = S.N, Nf = S.N_force;
   for (int base = warp * A; base < Na; base += NW * A) {
     const int il = base + aslot;
@@ -647,7 +653,7 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
       const double dx = (double)Fx - (double)S.force_ref[i];
       const double dy = (double)Fy - (double)S.force_ref[i + N];
       const double dz = (double)Fz - (double)S.force_ref[i + 2 * (size_t)N];
-      ferr += dx * dx + dy * dy + dz * dz;
+      ftab[(size_t)g * Na + il] = dx * dx + dy * dy + dz * dz;
       if (fdump && p < P) {
         fdump[((size_t)p * 3 + 0) * Nf + i] = Fx;
         fdump[((size_t)p * 3 + 1) * Nf + i] = Fy;
@@ -655,11 +661,33 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
       }
     }
   }
-  __syncthreads();  // the fold overwrites the f_ij scratch
+  __syncthreads();  // every atom's squared error is in the table
+  // Canonical sum of each individual's squared force errors: chunks of 32 consecutive atoms
+  // (a butterfly, lane 0's order; chunk sums spread over all warps and stored in place of the
+  // chunk's first entry), then the chunk sums in atom order.  The result does not depend on G,
+  // the block shape or the staging, so every force-item tiling gives the same bits.
+  const int nq = (Na + 31) >> 5;
+  for (int t = warp; t < G * nq; t += NW) {
+    const int gg = t / nq, q = t - gg * nq;
+    double* row = ftab + (size_t)gg * Na + 32 * q;
+    double v = 32 * q + lane < Na ? row[lane] : 0.0;
 #pragma unroll
-  for (int k = 0; k < 7; ++k) red[k * BLK + threadIdx.x] = 0.0;
-  red[7 * BLK + threadIdx.x] = ferr;
-  fold_item<GT>(it, P, S.Nc, red, res);
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncwarp();
+    if (lane == 0) row[0] = v;
+  }
+  __syncthreads();
+  for (int gg = threadIdx.x; gg < G; gg += BLK) {
+    double acc = 0.0;
+    for (int q = 0; q < nq; ++q) acc += ftab[(size_t)gg * Na + 32 * q];
+    const int pp = it.p0 + gg;
+    if (pp < P) {
+      double* r = res + ((size_t)pp * S.Nc + c) * kResK;
+#pragma unroll
+      for (int k = 0; k < 7; ++k) r[k] = 0.0;
+      r[7] = acc;
+    }
+  }
 }
 
 // Energy/virial Tersoff items read their geometry through L1: staging it in shared memory
@@ -1192,6 +1220,20 @@ constexpr int kBlockEV = 128;
 constexpr size_t kSmemMax = 220 * 1024;
 
 int zclass_of(int z) { return tersoff_zclass(z); }
+}  // namespace
+
+const char* tile_mode_name(int m) {
+  switch (m) {
+    case kTileDefault: return "default";
+    case kTileHalf: return "half-G";
+    case kTileQuarter: return "quarter-G";
+    case kTileGlobal: return "global-32";
+    case kTileUnstaged: return "unstaged";
+    default: return "?";
+  }
+}
+
+namespace {
 int nmax_of(int n) { return n <= 8 ? 8 : (n <= 16 ? 16 : (n <= 32 ? 32 : 0)); }
 }  // namespace
 
@@ -1312,8 +1354,11 @@ static bool tersoff_consts_exact(const PotentialSpec& sp, int num_types) {
 //     RI:      per pair of an active type 20 flops + 1 exp, cation-anion pairs 20 more + 2 exp
 //              (Morse); the linear terms are FP64 sums formed once per training set
 //     NN2B:    4n^2 + 13n + 10 flops + 2n tanh per pair
+// modes: per configuration the force-item tile (TileMode; empty: the default rule for all);
+// only: when given, the configurations whose items are built (the autotuner's trial launches).
 int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<ItemSpec>>& groups,
-              std::map<LaunchKey, size_t>& smem_need, size_t* gscratch_floats) {
+              std::map<LaunchKey, size_t>& smem_need, size_t* gscratch_floats, const std::vector<int8_t>* modes,
+              const std::vector<char>* only) {
   *gscratch_floats = 0;
   const DevSet& d = e->d;
   const TrainingSet& ts = e->ts;
@@ -1363,9 +1408,10 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
     }
   }
   for (int c = 0; c < ts.Nc; ++c) {
+    if (only && !(*only)[c]) continue;
     const bool force = c < ts.Nc_force;
     const int Na = ts.Na[c];
-    const long long Bc = (long long)e->h_off[ts.Na_sum[c] + Na] - e->h_off[ts.Na_sum[c]];
+    const int mode = (modes && !modes->empty() && (*modes)[c] > 0) ? (*modes)[c] : kTileDefault;
     int zc = 0, G = 32;
     size_t smem = kRedBytes;
     bool staged = false, global = false;
@@ -1384,22 +1430,26 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
           ((size_t)zc * Na * (16 + (d64 ? 8 : 4) + 1 + (force ? 4 : 0)) + (size_t)Na * 4 + 15) & ~(size_t)15;
       const size_t per_ind = (size_t)e->h_zmax[c] * Na * 3 * sizeof(float);  // slot-major, padded to max Z
       // force items: the constants table (tersoff_table_bytes), the f_ij scratch, the staged geometry
-      auto scratch = [&](int g) { return tersoff_table_bytes(g) + ((per_ind * g + 15) & ~(size_t)15); };
-      if (force && scratch(1) > force_smem_target(zc)) {
-        // not even one individual's scratch fits: 32 individuals per item (lane = individual,
-        // coalesced scratch rows) with the scratch in global memory
+      auto scratch = [&](int g) {
+        return tersoff_table_bytes(g) + tersoff_ferr_bytes(g, Na) + ((per_ind * g + 15) & ~(size_t)15);
+      };
+      if (force && (scratch(1) > force_smem_target(zc) || mode == kTileGlobal)) {
+        // 32 individuals per item (lane = individual, one atom per warp step, coalesced scratch
+        // rows) with the scratch (ZC slots) and the squared-error table in global memory: the
+        // only tile when not even one individual's scratch fits shared memory
         global = true;
-        item_floats = ((per_ind / sizeof(float)) * 32 + 63) & ~(size_t)63;
+        item_floats = ((size_t)zc * Na * 3 * 32 + (size_t)2 * Na * 32 + 63) & ~(size_t)63;
         smem = std::max(smem, kRedBytes + tersoff_table_bytes(32));
       } else if (force) {
+        // default rule: the largest G whose scratch fits, and the geometry staged too when it fits
+        // beside the scratch of >= 4 individuals
         while (G > 1 && scratch(G) > force_smem_target(zc)) G >>= 1;
-        // stage the geometry too when it fits beside the scratch of >= 4 individuals
         int Gs = G;
         while (Gs > 4 && scratch(Gs) + stage > stage_target(zc)) Gs >>= 1;
-        if (scratch(Gs) + stage <= stage_target(zc)) {
-          G = Gs;
-          staged = true;
-        }
+        if (scratch(Gs) + stage <= stage_target(zc)) G = Gs;
+        if (mode == kTileHalf) G = std::max(1, G / 2);
+        if (mode == kTileQuarter) G = std::max(1, G / 4);
+        staged = mode != kTileUnstaged && scratch(G) + stage <= stage_target(zc);
         fbytes = (per_ind * G + 15) & ~(size_t)15;
         smem = std::max(smem, scratch(G) + (staged ? stage : 0));
       } else {
@@ -1506,7 +1556,7 @@ int launch_one(const LaunchSet* ls, const Launch& L, cudaStream_t st, bool confi
 }  // namespace
 
 int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSet* ls,
-                    const std::vector<std::pair<const float*, double*>>* targets) {
+                    const std::vector<std::pair<const float*, double*>>* targets, const std::vector<char>* only) {
   std::map<LaunchKey, std::vector<ItemSpec>> groups;
   std::map<LaunchKey, size_t> smem_need;
   std::vector<int2> indmap;
@@ -1515,7 +1565,7 @@ int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSe
     Engine* e = jobs[j].first;
     Plan* plan = jobs[j].second;
     size_t need = 0;
-    GPUGA_TRY(job_items(e, plan->P, (int)j, groups, smem_need, &need));
+    GPUGA_TRY(job_items(e, plan->P, (int)j, groups, smem_need, &need, &plan->tiles, only));
     if (need > plan->gscratch_floats) {
       GPUGA_TRY(e->alloc(&plan->d_gscratch, need));
       plan->gscratch_floats = need;
@@ -1631,6 +1681,82 @@ int launchset_enqueue(LaunchSet* ls, cudaStream_t st) {
   return GPUGA_OK;
 }
 
+namespace {
+
+__global__ void fill_value(float* __restrict__ p, size_t n, float v) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+// Device time (ms) of the force launches of the configurations in `only`, with the plan's current
+// tiles: the best of three launches after one warm-up, on `st`.
+int time_force_items(Engine* e, Plan* plan, const std::vector<char>& only, cudaStream_t st, double* ms) {
+  LaunchSet ls;
+  GPUGA_TRY(launchset_build({{e, plan}}, &ls, nullptr, &only));
+  const int total = ls.total_individuals;
+  decode_jobs<<<(total + 127) / 128, 128, 0, st>>>(ls.d_jobs, ls.d_indmap, total);
+  GPUGA_CUDA(cudaGetLastError());
+  cudaEvent_t a = nullptr, b = nullptr;
+  GPUGA_CUDA(cudaEventCreate(&a));
+  GPUGA_CUDA(cudaEventCreate(&b));
+  double best = 1e30;
+  int s = GPUGA_OK;
+  for (int r = 0; r < 4 && s == GPUGA_OK; ++r) {
+    cudaEventRecord(a, st);
+    for (const Launch& L : ls.launches)
+      if (s == GPUGA_OK) s = launch_one(&ls, L, st, false);
+    cudaEventRecord(b, st);
+    const cudaError_t ce = cudaEventSynchronize(b);
+    if (ce != cudaSuccess) s = cuda_status(ce, "cudaEventSynchronize", __FILE__, __LINE__);
+    float t = 0.f;
+    if (s == GPUGA_OK) cudaEventElapsedTime(&t, a, b);
+    if (r > 0) best = std::min(best, (double)t);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = best;
+  return s;
+}
+
+// The autotuner: per size of force configuration (their atom count), time the force items of those
+// configurations under every tile (TileMode) on the first plan of a population size, and keep the
+// fastest; a tile replaces the default rule only when it is at least 3 % faster (timing noise).
+// Tiles never change a result bit, so the choice is free to follow the clock.
+int tune_tiles(Engine* e, Plan* plan) {
+  const TrainingSet& ts = e->ts;
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaStream_t st = e->stream;
+  const size_t npop = (size_t)plan->P * e->d.num_vars;
+  fill_value<<<(unsigned)((npop + 255) / 256), 256, 0, st>>>(plan->d_pop, npop, 0.5f);  // mid-range individuals
+  GPUGA_CUDA(cudaGetLastError());
+  std::map<int, std::vector<int>> classes;
+  for (int c = 0; c < ts.Nc_force; ++c) classes[ts.Na[c]].push_back(c);
+  plan->tiles.assign(ts.Nc, 0);
+  for (int c = 0; c < ts.Nc_force; ++c) plan->tiles[c] = kTileDefault;
+  for (const auto& kv : classes) {
+    std::vector<char> only(ts.Nc, 0);
+    for (int c : kv.second) only[c] = 1;
+    int best_mode = kTileDefault;
+    double best_ms = 0.0, default_ms = 0.0;
+    for (int mode : {kTileDefault, kTileHalf, kTileQuarter, kTileGlobal, kTileUnstaged}) {
+      for (int c : kv.second) plan->tiles[c] = (int8_t)mode;
+      double ms = 0.0;
+      GPUGA_TRY(time_force_items(e, plan, only, st, &ms));
+      if (mode == kTileDefault) {
+        default_ms = best_ms = ms;
+      } else if (ms < best_ms && ms < 0.97 * default_ms) {
+        best_ms = ms;
+        best_mode = mode;
+      }
+    }
+    for (int c : kv.second) plan->tiles[c] = (int8_t)best_mode;
+  }
+  plan->tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return GPUGA_OK;
+}
+
+}  // namespace
+
 int plan_build(Engine* e, int P, Plan** out) {
   const DevSet& d = e->d;
   std::unique_ptr<Plan> plan(new Plan);
@@ -1646,6 +1772,24 @@ int plan_build(Engine* e, int P, Plan** out) {
   GPUGA_TRY(e->alloc(&plan->d_pop, (size_t)P * d.num_vars));
   GPUGA_CUDA(cudaMallocHost(&plan->h_pop, sizeof(float) * (size_t)P * d.num_vars));
   GPUGA_CUDA(cudaMallocHost(&plan->h_fit, sizeof(double) * 4 * (size_t)P));
+  const bool tersoff = d.potential_type == 1 || d.potential_type == 2;
+  const int tiles = e->opt.tiles;
+  if (tersoff && tiles == 0 && e->ts.Nc_force > 0) {
+    GPUGA_TRY(tune_tiles(e, plan.get()));
+    // the trial launches may have grown the global scratch beyond what the chosen tiles need
+    if (plan->d_gscratch) {
+      GPUGA_CUDA(cudaStreamSynchronize(e->stream));
+      e->dfree(plan->d_gscratch);
+      plan->d_gscratch = nullptr;
+      plan->gscratch_floats = 0;
+    }
+  } else if (tersoff && tiles >= kTileDefault && tiles <= kTileUnstaged) {
+    plan->tiles.assign(e->ts.Nc, 0);
+    for (int c = 0; c < e->ts.Nc_force; ++c) plan->tiles[c] = (int8_t)tiles;
+  } else if (tiles < 0 || tiles > kTileUnstaged) {
+    set_error("gpuga_options.tiles must be 0..5 (got %d).", tiles);
+    return GPUGA_ERR_ARG;
+  }
   plan->ls.reset(new LaunchSet);
   GPUGA_TRY(launchset_build({{e, plan.get()}}, plan->ls.get()));
   *out = plan.release();

@@ -49,6 +49,7 @@ void gpuga_default_options(gpuga_options* opt) {
   opt->nn2b_r1 = 7.0f;
   opt->nn2b_r2 = 8.0f;
   opt->verbose = 0;
+  opt->tiles = 0;
 }
 
 const char* gpuga_last_error(void) { return last_error(); }
@@ -273,6 +274,17 @@ int gpuga_plan_info(gpuga_engine* h, int P, int* n_launches, double* per_launch,
       o[7] = ls->t_count ? ls->t_ms[k] / ls->t_count : 0.0;
     }
   }
+  return GPUGA_OK;
+}
+
+int gpuga_plan_tiles(gpuga_engine* h, int P, int* tiles, int cap, double* tune_ms) {
+  CHECK_ARG(h && P > 0, "gpuga_plan_tiles: invalid argument");
+  Plan* plan = nullptr;
+  GPUGA_CUDA(cudaSetDevice(h->e->device));
+  const int s = plan_get(h->e, P, &plan);
+  if (s != GPUGA_OK) return s;
+  for (int c = 0; tiles && c < cap && c < h->e->d.Nc; ++c) tiles[c] = c < (int)plan->tiles.size() ? plan->tiles[c] : 0;
+  if (tune_ms) *tune_ms = plan->tune_ms;
   return GPUGA_OK;
 }
 

@@ -26,8 +26,18 @@ int Engine::dalloc(void** p, size_t bytes) {
     return cuda_status(err, "cudaMalloc", __FILE__, __LINE__);
   }
   allocations.push_back(*p);
+  allocation_bytes[*p] = bytes;
   device_bytes += bytes;
   return GPUGA_OK;
+}
+
+void Engine::dfree(void* p) {
+  auto it = std::find(allocations.begin(), allocations.end(), p);
+  if (it == allocations.end()) return;
+  allocations.erase(it);
+  device_bytes -= allocation_bytes[p];
+  allocation_bytes.erase(p);
+  cudaFree(p);
 }
 
 namespace {

@@ -189,6 +189,19 @@ struct LaunchSet {
   ~LaunchSet();
 };
 
+// Tile of a Tersoff force configuration's work items: individuals per item G and where the
+// f_ij scratch and geometry live (batched.cu, job_items).  Every tile gives the same results bit
+// for bit (same per-atom arithmetic, canonical force-error sum); the autotuner picks per
+// configuration size.
+enum TileMode {
+  kTileDefault = 1,   // the largest G whose scratch fits shared memory, geometry staged when it fits
+  kTileHalf = 2,      // half that G (staged when it fits)
+  kTileQuarter = 3,   // a quarter of it
+  kTileGlobal = 4,    // 32 individuals, scratch in global memory
+  kTileUnstaged = 5,  // the default G, geometry read from the slot-major global copy
+};
+const char* tile_mode_name(int m);
+
 // Per (engine, population size) buffers plus the engine's own launch set.
 struct Plan {
   int P = 0;
@@ -208,6 +221,8 @@ struct Plan {
   bool dump = false;           // pass d_fdump to the kernels (eager launches only)
   cudaGraphExec_t graph = nullptr;
   std::unique_ptr<LaunchSet> ls;
+  std::vector<int8_t> tiles;   // per configuration: the force-item TileMode (empty: default rule)
+  double tune_ms = 0;          // host time the autotuner took
   ~Plan();
 };
 
@@ -224,6 +239,7 @@ struct Engine {
   std::map<int, std::unique_ptr<Plan>> plans;    // keyed by population size
   size_t device_bytes = 0;
   std::vector<void*> allocations;
+  std::map<void*, size_t> allocation_bytes;
   // plain-path scratch
   double* s64 = nullptr;  // per-bond scratch (S, A, f_ij x/y/z) FP64
   float* s32 = nullptr;
@@ -239,6 +255,7 @@ struct Engine {
   size_t p_w_bytes = 0;
   ~Engine();
   int dalloc(void** p, size_t bytes);
+  void dfree(void* p);  // frees an allocation made by dalloc before the engine's end
   template <class T>
   int alloc(T** p, size_t n) {
     return dalloc(reinterpret_cast<void**>(p), n * sizeof(T));
@@ -276,7 +293,8 @@ JobView make_job_view(const Engine* e, const Plan* plan);
 // Builds the shared launches of the given jobs (one engine + plan each); `targets`, when given,
 // names each job's population and fitness buffers (default: the plan's own).
 int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSet* ls,
-                    const std::vector<std::pair<const float*, double*>>* targets = nullptr);
+                    const std::vector<std::pair<const float*, double*>>* targets = nullptr,
+                    const std::vector<char>* only = nullptr);
 // Enqueues one generation of every job of the set on `st` (force launches on a side stream).
 int launchset_enqueue(LaunchSet* ls, cudaStream_t st);
 int launchset_collect_timing(LaunchSet* ls);

@@ -193,6 +193,9 @@ int gpuga_server::setup(Job* j) {
     gpuga_options opt;
     gpuga_default_options(&opt);
     opt.device = device;
+    // the fixed tile rule: trial launches timed on a GPU that runs other jobs' windows would
+    // measure the contention, not the tiles (every tile gives the same results)
+    opt.tiles = kTileDefault;
     Engine* e = nullptr;
     GPUGA_TRY(engine_create(j->spec, std::move(j->ts), opt, &e));
     j->engine = e;

@@ -22,13 +22,14 @@ def _p(a: np.ndarray):
 
 def options(device: int = 0, path: int = PATH_BATCHED, use_graph: bool = True, nn2b_consistent: bool = False,
             nn2b_r1: float = 7.0, nn2b_r2: float = 8.0, verbose: bool = False, neighbor_cells: int = 0,
-            ri_self_energy: bool = False) -> _lib.Options:
+            ri_self_energy: bool = False, tiles: int = 0) -> _lib.Options:
     o = _lib.Options()
     _lib.load().gpuga_default_options(C.byref(o))
     o.device, o.path, o.use_graph = device, path, int(use_graph)
     o.nn2b_consistent, o.nn2b_r1, o.nn2b_r2, o.verbose = int(nn2b_consistent), nn2b_r1, nn2b_r2, int(verbose)
     o.neighbor_cells = neighbor_cells
     o.ri_self_energy = int(ri_self_energy)
+    o.tiles = tiles
     return o
 
 
@@ -142,6 +143,13 @@ class Fitness:
         """Fitness::predict (fitness.cu:335-390): writes force.out, energy.out, virial.out."""
         e = np.ascontiguousarray(elite, np.float32)
         check(_lib.load().gpuga_predict(self._h, input_dir.encode(), _p(e)))
+
+    def plan_tiles(self, population_size: int):
+        """(per-configuration force-item tile codes, autotuner host time in ms) of the plan for P."""
+        t = np.zeros(self.Nc, np.int32)
+        ms = C.c_double()
+        check(_lib.load().gpuga_plan_tiles(self._h, population_size, _p(t), self.Nc, C.byref(ms)))
+        return t, ms.value
 
     def neighbors(self):
         """(NN[N], nbr[num_bonds]) in CSR form, ascending neighbor indices."""

@@ -59,6 +59,11 @@ typedef struct gpuga_options {
   int ri_self_energy;  /* RI (potential types 0 and 4): 1 subtracts the damped-Coulomb self energy
                           -K_C sum_i q_i^2 [alpha/sqrt(pi) + erfc(alpha rc)/rc + alpha/sqrt(pi) exp(-alpha^2 rc^2)]
                           from every atom's energy, in FP64; 0 (default) keeps ri.cu, which has none */
+  int tiles;           /* Tersoff force-item tiles: 0 (default) autotuned per configuration size when a
+                          population plan is built, 1 the fixed rule (the largest individuals-per-item
+                          count whose scratch fits shared memory), 2 half of it, 3 a quarter, 4 32
+                          individuals with the scratch in global memory, 5 the fixed rule without staged
+                          geometry.  Every choice gives bit-identical results. */
 } gpuga_options;
 
 /* Fills *opt with the reference's semantics (batched path, graphs on, NN2B taper 7..8 A, force quirk kept). */
@@ -134,6 +139,10 @@ int gpuga_batched_forces(gpuga_engine* e, int P, const float* pop01, float* forc
  * per_launch (may be NULL) receives up to `cap` rows of 8 doubles:
  * {kind (0 Tersoff, 1 RI, 2 NN2B), register class, force items?, CTAs, (individual, atom) units,
  *  algorithmic FP32 flops, transcendental calls, mean device ms per generation while timing is on}. */
+/* The force-item tile of every configuration (tiles[Nc], gpuga_options.tiles codes 1-5; 0 for
+ * energy/virial and non-Tersoff configurations) of the plan for population size P, and the host time
+ * the autotuner spent on it. */
+int gpuga_plan_tiles(gpuga_engine* e, int P, int* tiles, int cap, double* tune_ms);
 int gpuga_plan_info(gpuga_engine* e, int P, int* n_launches, double* per_launch, int cap);
 /* Records CUDA events around every batched launch of population size P (eager launches only:
  * gpuga_fitness_device, or gpuga_fitness with use_graph = 0).  While timing is on, the launches
