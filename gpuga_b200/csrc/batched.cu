@@ -546,8 +546,15 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
 // ST: staged (1) or in-place CSR (0) geometry, or decided per item (-1).
 // Bytes of the force items' shared-memory table of per-individual constants (G entries).
 __host__ __device__ constexpr size_t tersoff_table_bytes(int G) { return ((size_t)G * sizeof(TersoffC) + 15) & ~(size_t)15; }
-// Bytes of the force items' table of per-(individual, atom) squared force errors.
-__host__ __device__ constexpr size_t tersoff_ferr_bytes(int G, int Na) { return ((size_t)G * Na * sizeof(double) + 15) & ~(size_t)15; }
+// The per-(individual, atom) squared force errors of a force item: row g holds the item's atoms
+// in chunks of 32, each chunk padded by one double (consecutive chunks start in different banks).
+// Shared-memory items keep them in the f_ij scratch once every f_ij has been read; an item with
+// its scratch in global memory keeps them after it.
+__host__ __device__ constexpr int ferr_row(int Na) { return Na + ((Na + 31) >> 5); }
+__host__ __device__ constexpr int ferr_pos(int il) { return il + (il >> 5); }
+// Atoms per thread in a shared-memory force item's gather pass, at most: their squared errors
+// wait in registers until the scratch is free.  The host's G rule keeps Na * G <= 256 * this.
+__host__ __device__ constexpr int ferr_steps(int zc) { return zc == 4 ? 6 : (zc == 8 ? 4 : 2); }
 
 // Pair-term form of the two kinds of Tersoff items (tersoff_atom, PairMode).  Energy/virial items
 // take the FP64 pair terms: the configuration virial sums the radial forces of all bonds, whose
@@ -583,14 +590,11 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
   TersoffC* ctab = reinterpret_cast<TersoffC*>(smem);
   if (FORCE && warp == 0 && aslot == 0) ctab[g] = Creg;
   // force scratch: shared memory, or for configurations too large for it the item's own
-  // region of global memory (visible to the whole CTA after __syncthreads as well); the
-  // per-(individual, atom) squared force errors ftab[g][il] before it (shared memory) or after
-  // it (global memory)
+  // region of global memory (visible to the whole CTA after __syncthreads as well)
   const bool glob = FORCE && item_global(it);
-  float* fsm = glob ? J.gscratch + (size_t)it.gofs * 64 : reinterpret_cast<float*>(smem + tab + tersoff_ferr_bytes(G, Na));
-  double* ftab = glob ? reinterpret_cast<double*>(fsm + (size_t)ZC * Na * 3 * 32) : reinterpret_cast<double*>(smem + tab);
+  float* fsm = glob ? J.gscratch + (size_t)it.gofs * 64 : reinterpret_cast<float*>(smem + tab);
   double* red = reinterpret_cast<double*>(smem);
-  const size_t front = FORCE ? tab + tersoff_ferr_bytes(G, Na) + item_fbytes(it) : (size_t)BLK * kResK * sizeof(double);
+  const size_t front = FORCE ? tab + item_fbytes(it) : (size_t)BLK * kResK * sizeof(double);
   if (FORCE) __syncthreads();  // the constants table
   const TersoffC& C = FORCE ? ctab[g] : Creg;
   if (!FORCE) {
@@ -632,61 +636,94 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
   }
   __syncthreads();
   const int N = S.N, Nf = S.N_force;
-  for (int base = warp * A; base < Na; base += NW * A) {
-    const int il = base + aslot;
-    if (il < Na) {
-      const int i = atom0 + il;
-      const int b0 = geo.base(il), bs = geo.step(), Z = geo.nn[il];
-      float Fx = 0.f, Fy = 0.f, Fz = 0.f;
-      int rls[ZC];
+  const int nq = (Na + 31) >> 5, NaP = ferr_row(Na);
+  // gather pass: F_i = sum_j (f_ij - f_ji) of (individual g, atom il) and its squared error
+  auto atom_error = [&](int il) -> double {
+    const int i = atom0 + il;
+    const int b0 = geo.base(il), bs = geo.step(), Z = geo.nn[il];
+    float Fx = 0.f, Fy = 0.f, Fz = 0.f;
+    int rls[ZC];
 #pragma unroll
-      for (int j = 0; j < ZC; ++j) rls[j] = j < Z ? geo.rev[b0 + j * bs] : 0;
+    for (int j = 0; j < ZC; ++j) rls[j] = j < Z ? geo.rev[b0 + j * bs] : 0;
 #pragma unroll
-      for (int j = 0; j < ZC; ++j) {
-        if (j < Z) {
-          const int bl = j * Na + il, rl = rls[j];
-          Fx += fsm[(bl * 3 + 0) * G + g] - fsm[(rl * 3 + 0) * G + g];
-          Fy += fsm[(bl * 3 + 1) * G + g] - fsm[(rl * 3 + 1) * G + g];
-          Fz += fsm[(bl * 3 + 2) * G + g] - fsm[(rl * 3 + 2) * G + g];
-        }
-      }
-      const double dx = (double)Fx - (double)S.force_ref[i];
-      const double dy = (double)Fy - (double)S.force_ref[i + N];
-      const double dz = (double)Fz - (double)S.force_ref[i + 2 * (size_t)N];
-      ftab[(size_t)g * Na + il] = dx * dx + dy * dy + dz * dz;
-      if (fdump && p < P) {
-        fdump[((size_t)p * 3 + 0) * Nf + i] = Fx;
-        fdump[((size_t)p * 3 + 1) * Nf + i] = Fy;
-        fdump[((size_t)p * 3 + 2) * Nf + i] = Fz;
+    for (int j = 0; j < ZC; ++j) {
+      if (j < Z) {
+        const int bl = j * Na + il, rl = rls[j];
+        Fx += fsm[(bl * 3 + 0) * G + g] - fsm[(rl * 3 + 0) * G + g];
+        Fy += fsm[(bl * 3 + 1) * G + g] - fsm[(rl * 3 + 1) * G + g];
+        Fz += fsm[(bl * 3 + 2) * G + g] - fsm[(rl * 3 + 2) * G + g];
       }
     }
-  }
-  __syncthreads();  // every atom's squared error is in the table
-  // Canonical sum of each individual's squared force errors: chunks of 32 consecutive atoms
-  // (a butterfly, lane 0's order; chunk sums spread over all warps and stored in place of the
-  // chunk's first entry), then the chunk sums in atom order.  The result does not depend on G,
-  // the block shape or the staging, so every force-item tiling gives the same bits.
-  const int nq = (Na + 31) >> 5;
-  for (int t = warp; t < G * nq; t += NW) {
-    const int gg = t / nq, q = t - gg * nq;
-    double* row = ftab + (size_t)gg * Na + 32 * q;
-    double v = 32 * q + lane < Na ? row[lane] : 0.0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    __syncwarp();
-    if (lane == 0) row[0] = v;
-  }
-  __syncthreads();
-  for (int gg = threadIdx.x; gg < G; gg += BLK) {
-    double acc = 0.0;
-    for (int q = 0; q < nq; ++q) acc += ftab[(size_t)gg * Na + 32 * q];
-    const int pp = it.p0 + gg;
-    if (pp < P) {
-      double* r = res + ((size_t)pp * S.Nc + c) * kResK;
-#pragma unroll
-      for (int k = 0; k < 7; ++k) r[k] = 0.0;
-      r[7] = acc;
+    const double dx = (double)Fx - (double)S.force_ref[i];
+    const double dy = (double)Fy - (double)S.force_ref[i + N];
+    const double dz = (double)Fz - (double)S.force_ref[i + 2 * (size_t)N];
+    if (fdump && p < P) {
+      fdump[((size_t)p * 3 + 0) * Nf + i] = Fx;
+      fdump[((size_t)p * 3 + 1) * Nf + i] = Fy;
+      fdump[((size_t)p * 3 + 2) * Nf + i] = Fz;
     }
+    return dx * dx + dy * dy + dz * dz;
+  };
+  // Canonical sum of each individual's squared force errors: every chunk of 32 consecutive atoms
+  // summed in atom order by one thread (tasks = G * nq <= BLK for shared-memory items), the
+  // chunk sum stored over the chunk's first entry, then the chunk sums in atom order.  The result
+  // depends on neither G, nor the block shape, nor the staging, so every force-item tiling gives
+  // the same bits.
+  auto fold = [&](double* ftab) {
+    for (int t = threadIdx.x; t < G * nq; t += BLK) {
+      const int gg = t / nq, q = t - gg * nq;
+      double* row = ftab + gg * NaP + 33 * q;
+      const int m = min(32, Na - 32 * q);
+      double acc = 0.0;
+#pragma unroll 4
+      for (int k = 0; k < m; ++k) acc += row[k];
+      row[0] = acc;
+    }
+    __syncthreads();
+    for (int gg = threadIdx.x; gg < G; gg += BLK) {
+      double acc = 0.0;
+      for (int q = 0; q < nq; ++q) acc += ftab[gg * NaP + 33 * q];
+      const int pp = it.p0 + gg;
+      if (pp < P) {
+        double* r = res + ((size_t)pp * S.Nc + c) * kResK;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) r[k] = 0.0;
+        r[7] = acc;
+      }
+    }
+  };
+  if (glob) {
+    double* ftab = reinterpret_cast<double*>(fsm + (size_t)ZC * Na * 3 * 32);
+    for (int base = warp * A; base < Na; base += NW * A) {
+      const int il = base + aslot;
+      if (il < Na) ftab[g * NaP + ferr_pos(il)] = atom_error(il);
+    }
+    __syncthreads();
+    fold(ftab);
+  } else {
+    // the errors wait in registers (at most ferr_steps per thread, by the host's G rule) until
+    // every f_ij has been read, then take the scratch's place
+    constexpr int KS = ferr_steps(ZC);
+    if (Na > KS * NW * A) {  // outside the host's G rule: a NaN fitness rather than a wrong one
+      for (int gg = threadIdx.x; gg < G; gg += BLK)
+        if (it.p0 + gg < P) res[((size_t)(it.p0 + gg) * S.Nc + c) * kResK + 7] = __longlong_as_double(0x7ff8000000000000LL);
+      return;
+    }
+    double ev[KS];
+#pragma unroll
+    for (int k = 0; k < KS; ++k) {
+      const int il = (warp + k * NW) * A + aslot;
+      ev[k] = il < Na ? atom_error(il) : 0.0;
+    }
+    __syncthreads();
+    double* ftab = reinterpret_cast<double*>(smem + tab);
+#pragma unroll
+    for (int k = 0; k < KS; ++k) {
+      const int il = (warp + k * NW) * A + aslot;
+      if (il < Na) ftab[g * NaP + ferr_pos(il)] = ev[k];
+    }
+    __syncthreads();
+    fold(ftab);
   }
 }
 
@@ -858,12 +895,21 @@ struct NNSmem {
   }
 };
 
+// How nn_pairs forms the pair energy p2 = sum_a w2_a tanh(x2_a - b1_a) - b2.  Near a fitted
+// optimum the sum and b2 cancel: most pairs lie near the cutoff, where the network's output
+// must be small, while its terms are of the size of w2.  The FP32 rounding of those terms and
+// partial sums (eps |w2|, coherent over the pairs of a shell) then set the fitness error of
+// the best individuals (1e-5 relative at fitness 0.04 on the 10-neuron set).  Each product of
+// two floats is exact in FP64, so an FP64 sum of the terms leaves only the FP32 errors of
+// x2t itself, which do not cancel.  The force needs p2 only inside the taper shell (fcp != 0):
+// `with_p2` (warp-uniform) skips it elsewhere.
+
 // NP pairs of the same lane at once: every weight loaded from shared memory
 // feeds the NP pairs (the hidden-to-hidden loads, not the FMAs, bound a
 // single pair).  Each pair's arithmetic is the same sequence as for NP = 1.
 template <int NMAX, int NP, bool FULL>
 __device__ __forceinline__ void nn_pairs(const float* __restrict__ wsm, int lane, int n, const float (&d)[NP],
-                                         float (&p2)[NP], float (&f2)[NP]) {
+                                         bool with_p2, float (&p2)[NP], float (&f2)[NP]) {
   if (FULL) n = NMAX;  // every row present: the row loop unrolls completely
   constexpr int Q = NMAX / 4;
   const float4* W1 = reinterpret_cast<const float4*>(wsm);
@@ -883,8 +929,12 @@ __device__ __forceinline__ void nn_pairs(const float* __restrict__ wsm, int lane
         y1[u][4 * q + c] = (1.0f - x1[u][4 * q + c] * x1[u][4 * q + c]) * w0c[c];
       }
   }
+  double p2d[NP];
 #pragma unroll
-  for (int u = 0; u < NP; ++u) p2[u] = f2[u] = 0.f;
+  for (int u = 0; u < NP; ++u) {
+    p2[u] = f2[u] = 0.f;
+    p2d[u] = 0.0;
+  }
   const int qa_end = (n + 3) >> 2;
 #pragma unroll (FULL ? NMAX / 4 : 1)
   for (int qa = 0; qa < qa_end; ++qa) {
@@ -917,14 +967,14 @@ __device__ __forceinline__ void nn_pairs(const float* __restrict__ wsm, int lane
         for (int u = 0; u < NP; ++u) {
           const float x2t = tanhf(x2[u] - b1c[c]);
           const float y2t = y2[u] * (1.0f - x2t * x2t);
-          p2[u] = fmaf(w2c[c], x2t, p2[u]);
+          if (with_p2) p2d[u] = fma((double)w2c[c], (double)x2t, p2d[u]);
           f2[u] = fmaf(w2c[c], y2t, f2[u]);
         }
       }
     }
   }
 #pragma unroll
-  for (int u = 0; u < NP; ++u) p2[u] -= b2;
+  for (int u = 0; u < NP; ++u) p2[u] = with_p2 ? (float)(p2d[u] - (double)b2) : 0.f;
 }
 
 // RI: three CTAs per SM (at most 85 registers); NN2B: two (128 registers, two pairs per
@@ -1130,10 +1180,15 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
           q[u] = __ldg(&S.g32[min(b + u, bend - 1)]);
           d[u] = q[u].w;
         }
+        // force items: p2 enters only through the taper derivative (warp-uniform test: the
+        // 32 lanes share the pairs)
+        bool need_p2 = !FORCE;
+#pragma unroll
+        for (int u = 0; u < NP; ++u) need_p2 |= d[u] >= tp.r1;
         if (nn == NMAX)
-          nn_pairs<NMAX, NP, true>(wsm, lane, nn, d, p2, f2raw);
+          nn_pairs<NMAX, NP, true>(wsm, lane, nn, d, need_p2, p2, f2raw);
         else
-          nn_pairs<NMAX, NP, false>(wsm, lane, nn, d, p2, f2raw);
+          nn_pairs<NMAX, NP, false>(wsm, lane, nn, d, need_p2, p2, f2raw);
 #pragma unroll
         for (int u = 0; u < NP; ++u) {
           if (b + u < bend) {
@@ -1234,7 +1289,8 @@ const char* tile_mode_name(int m) {
 }
 
 namespace {
-int nmax_of(int n) { return n <= 8 ? 8 : (n <= 16 ? 16 : (n <= 32 ? 32 : 0)); }
+// register classes of the NN2B MLP width (12 covers the reference's largest width, 10)
+int nmax_of(int n) { return n <= 8 ? 8 : (n <= 12 ? 12 : (n <= 16 ? 16 : (n <= 32 ? 32 : 0))); }
 }  // namespace
 
 DevView make_view(const DevSet& d) {
@@ -1321,8 +1377,6 @@ Plan::~Plan() {
   if (h_fit) cudaFreeHost(h_fit);
 }
 
-namespace {
-
 struct ItemSpec {
   WorkItem w;
   double cost, units, flops, sfu;
@@ -1333,6 +1387,14 @@ struct LaunchKey {
     return std::tie(kind, zclass, nmax, force, lo) < std::tie(o.kind, o.zclass, o.nmax, o.force, o.lo);
   }
 };
+// A plan's work items grouped by launch (job index 0), with their shared-memory and global-scratch needs.
+struct ItemCache {
+  std::map<LaunchKey, std::vector<ItemSpec>> groups;
+  std::map<LaunchKey, size_t> smem_need;
+  size_t need = 0;
+};
+
+namespace {
 
 // True when every derived Tersoff constant of every individual is exact in FP32: S fixed at 2 by
 // its bounds, so that lr = 2A, la = A, cr = D0, ca = 2 D0 are FP32 parameters times powers of two.
@@ -1428,22 +1490,27 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
       const bool d64 = (force ? kPairModeForce : kPairModeEV) == kPair64;
       const size_t stage =
           ((size_t)zc * Na * (16 + (d64 ? 8 : 4) + 1 + (force ? 4 : 0)) + (size_t)Na * 4 + 15) & ~(size_t)15;
-      const size_t per_ind = (size_t)e->h_zmax[c] * Na * 3 * sizeof(float);  // slot-major, padded to max Z
+      // per individual: the f_ij scratch (slot-major, padded to max Z), which afterwards holds the
+      // squared-error rows (ferr_row)
+      const size_t per_ind = std::max((size_t)e->h_zmax[c] * Na * 3 * sizeof(float),
+                                      (size_t)ferr_row(Na) * sizeof(double));
       // force items: the constants table (tersoff_table_bytes), the f_ij scratch, the staged geometry
-      auto scratch = [&](int g) {
-        return tersoff_table_bytes(g) + tersoff_ferr_bytes(g, Na) + ((per_ind * g + 15) & ~(size_t)15);
+      auto scratch = [&](int g) { return tersoff_table_bytes(g) + ((per_ind * g + 15) & ~(size_t)15); };
+      // the gather pass holds at most ferr_steps(zc) atoms per thread (8 warps of 32 / g atoms)
+      auto fits = [&](int g) {
+        return scratch(g) <= force_smem_target(zc) && (size_t)Na * g <= (size_t)ferr_steps(zc) * kBlock;
       };
-      if (force && (scratch(1) > force_smem_target(zc) || mode == kTileGlobal)) {
+      if (force && (!fits(1) || mode == kTileGlobal)) {
         // 32 individuals per item (lane = individual, one atom per warp step, coalesced scratch
         // rows) with the scratch (ZC slots) and the squared-error table in global memory: the
         // only tile when not even one individual's scratch fits shared memory
         global = true;
-        item_floats = ((size_t)zc * Na * 3 * 32 + (size_t)2 * Na * 32 + 63) & ~(size_t)63;
+        item_floats = ((size_t)zc * Na * 3 * 32 + (size_t)2 * ferr_row(Na) * 32 + 63) & ~(size_t)63;
         smem = std::max(smem, kRedBytes + tersoff_table_bytes(32));
       } else if (force) {
         // default rule: the largest G whose scratch fits, and the geometry staged too when it fits
         // beside the scratch of >= 4 individuals
-        while (G > 1 && scratch(G) > force_smem_target(zc)) G >>= 1;
+        while (G > 1 && !fits(G)) G >>= 1;
         int Gs = G;
         while (Gs > 4 && scratch(Gs) + stage > stage_target(zc)) Gs >>= 1;
         if (scratch(Gs) + stage <= stage_target(zc)) G = Gs;
@@ -1541,6 +1608,8 @@ int launch_one(const LaunchSet* ls, const Launch& L, cudaStream_t st, bool confi
     if (L.force) GPUGA_PAIR(1, 8, true); else GPUGA_PAIR(1, 8, false);
   } else if (L.nmax == 8) {
     if (L.force) GPUGA_PAIR(2, 8, true); else GPUGA_PAIR(2, 8, false);
+  } else if (L.nmax == 12) {
+    if (L.force) GPUGA_PAIR(2, 12, true); else GPUGA_PAIR(2, 12, false);
   } else if (L.nmax == 16) {
     if (L.force) GPUGA_PAIR(2, 16, true); else GPUGA_PAIR(2, 16, false);
   } else {
@@ -1565,7 +1634,31 @@ int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSe
     Engine* e = jobs[j].first;
     Plan* plan = jobs[j].second;
     size_t need = 0;
-    GPUGA_TRY(job_items(e, plan->P, (int)j, groups, smem_need, &need, &plan->tiles, only));
+    // a plan's items depend only on its training set, population size and tiles: computed once
+    // (a pass over every atom and bond) and reused by every launch set the job joins
+    if (only || !plan->items) {
+      std::shared_ptr<ItemCache> cache(new ItemCache);
+      GPUGA_TRY(job_items(e, plan->P, 0, cache->groups, cache->smem_need, &cache->need, &plan->tiles, only));
+      if (!only) plan->items = cache;
+      for (auto& kv : cache->groups)
+        for (ItemSpec t : kv.second) {
+          t.w.job = (int)j;
+          groups[kv.first].push_back(t);
+        }
+      for (auto& kv : cache->smem_need) smem_need[kv.first] = std::max(smem_need[kv.first], kv.second);
+      need = cache->need;
+    } else {
+      const ItemCache& cache = *plan->items;
+      for (auto& kv : cache.groups) {
+        std::vector<ItemSpec>& dst = groups[kv.first];
+        for (ItemSpec t : kv.second) {
+          t.w.job = (int)j;
+          dst.push_back(t);
+        }
+      }
+      for (auto& kv : cache.smem_need) smem_need[kv.first] = std::max(smem_need[kv.first], kv.second);
+      need = cache.need;
+    }
     if (need > plan->gscratch_floats) {
       GPUGA_TRY(e->alloc(&plan->d_gscratch, need));
       plan->gscratch_floats = need;

@@ -202,6 +202,8 @@ enum TileMode {
 };
 const char* tile_mode_name(int m);
 
+struct ItemCache;  // batched.cu: a plan's work items, computed once
+
 // Per (engine, population size) buffers plus the engine's own launch set.
 struct Plan {
   int P = 0;
@@ -222,6 +224,7 @@ struct Plan {
   cudaGraphExec_t graph = nullptr;
   std::unique_ptr<LaunchSet> ls;
   std::vector<int8_t> tiles;   // per configuration: the force-item TileMode (empty: default rule)
+  std::shared_ptr<ItemCache> items;  // the work items of this plan (launchset_build)
   double tune_ms = 0;          // host time the autotuner took
   ~Plan();
 };

@@ -27,10 +27,13 @@
 //
 // Work items of different jobs never share a CTA and all reductions are
 // fixed-order, so a job's trajectory is identical alone and in any mix.
-// Latency is reported two ways: the device time of each generation of all
-// resident jobs, and per job and generation the wall-clock time between the
-// job's successive window harvests divided by the window's generations (every
-// stall -- rebuilds, admissions, frees -- included).  There is no counterpart
+// Latency is reported three ways: the device time of each generation of all
+// resident jobs; per job and generation the wall-clock time between the job's
+// successive window harvests divided by the window's generations (every stall
+// of a running job -- rebuilds, admissions of others, frees -- included; a
+// job's first window counts from its enqueue); and per job the time from
+// submission to the harvest of its first window (queueing, setup, the wait for
+// the window in flight and the first window itself).  There is no counterpart
 // in the reference, which fits one potential per process (main.cu:25-55).
 #include <algorithm>
 #include <chrono>
@@ -159,6 +162,7 @@ struct gpuga_server {
   // statistics
   std::vector<double> tick_ms;   // device time of each generation of all resident jobs
   std::vector<double> wall_ms;   // per job and generation: wall-clock time, stalls included
+  std::vector<double> first_ms;  // per job: submission to the harvest of its first window (wall clock)
   long batches = 0, finished = 0;
   double evals = 0, busy_s = 0;
   int peak_resident = 0;
@@ -300,6 +304,8 @@ int gpuga_server::harvest(const Window& w) {
   for (Job* j : w.batch->jobs) {
     const float* h = device_ga_history(j->dga.get(), w.b);
     for (int q = 0; q < w.n; ++q) j->best.push_back(h[(size_t)q * (j->ga.d + 1)]);
+    if (j->ga.generation == 0)
+      first_ms.push_back(std::chrono::duration<double, std::milli>(now - j->t_submit).count());
     j->ga.generation += w.n;
     evals += (double)j->plan->P * j->engine->d.N * w.n;
     const double per_gen = std::chrono::duration<double, std::milli>(now - j->t_mark).count() / w.n;
@@ -373,7 +379,11 @@ void gpuga_server::run() {
       if (s == GPUGA_OK) s = ga_batch_window(use->gab.get(), b, n, true, true, st);
       if (s == GPUGA_OK) {
         nxt = Window{use, b, n};
-        for (Job* j : next) j->gens_queued += n;
+        const auto t_enq = Clock::now();
+        for (Job* j : next) {
+          if (j->gens_queued == 0) j->t_mark = t_enq;  // its generations start behind window k
+          j->gens_queued += n;
+        }
       } else {
         status = s;
       }
@@ -621,7 +631,9 @@ int gpuga_server_stats(gpuga_server* s, double* out, int n) {
                       s->evals,
                       percentile(s->wall_ms, 0.50),
                       percentile(s->wall_ms, 0.99),
-                      s->busy_s};
+                      s->busy_s,
+                      percentile(s->first_ms, 0.50),
+                      percentile(s->first_ms, 0.99)};
   const int m = std::min(n, (int)(sizeof(v) / sizeof(v[0])));
   for (int k = 0; k < m; ++k) out[k] = v[k];
   return GPUGA_OK;

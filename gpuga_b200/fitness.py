@@ -210,7 +210,8 @@ class Server:
 
     def stats(self) -> dict:
         keys = ("batches", "jobs_finished", "p50_gen_ms", "p99_gen_ms", "evals_per_s", "device_bytes",
-                "peak_resident_jobs", "total_evals", "p50_wall_gen_ms", "p99_wall_gen_ms", "busy_s")
+                "peak_resident_jobs", "total_evals", "p50_wall_gen_ms", "p99_wall_gen_ms", "busy_s",
+                "p50_first_window_ms", "p99_first_window_ms")
         s = np.zeros(len(keys))
         check(_lib.load().gpuga_server_stats(self._h, _p(s), len(keys)))
         return dict(zip(keys, (float(v) for v in s)))

@@ -264,10 +264,12 @@ int gpuga_server_cancel(gpuga_server* s, int job_id);
 int gpuga_server_hold(gpuga_server* s, int on);
 /* Runs the scheduler until every submitted job is finished (or timeout_s elapses, -> GPUGA_ERR_TIMEOUT). */
 int gpuga_server_drain(gpuga_server* s, double timeout_s);
-/* Fills stats[0 .. n-1] (n <= 11) with: {generation batches run, jobs finished, p50 and p99 of the
+/* Fills stats[0 .. n-1] (n <= 13) with: {generation batches run, jobs finished, p50 and p99 of the
  *         device time of a generation of all resident jobs (ms), aggregate evals/s over the busy wall
  *         time, device bytes in use, peak jobs resident, total evals, p50 and p99 of the wall-clock time
- *         per generation as each job saw it (ms; every stall included), busy wall time (s)} */
+ *         per generation as each job saw it (ms; every stall of a running job included), busy wall
+ *         time (s), p50 and p99 of the time from a job's submission to the harvest of its first
+ *         window of generations (ms)} */
 int gpuga_server_stats(gpuga_server* s, double* stats, int n);
 int gpuga_server_destroy(gpuga_server* s);
 

@@ -63,6 +63,7 @@ def test_jobs_are_the_same_alone_and_in_the_mix(job_dirs):
         assert st["batches"] == GENS
         assert st["p99_gen_ms"] >= st["p50_gen_ms"] > 0
         assert st["p99_wall_gen_ms"] >= st["p50_wall_gen_ms"] > 0
+        assert st["p99_first_window_ms"] >= st["p50_first_window_ms"] > 0
         for jid, d, (best, elite) in zip(ids, job_dirs, refs):
             status, done, total, state = srv.poll(jid)
             assert (status, done, total, state) == (_lib.OK, GENS, GENS, Server.DONE)
