@@ -227,14 +227,19 @@ __device__ __forceinline__ void cutoff_fn(float r1, float r2, float pf, float d,
 
 // WorkItem::G packs the individuals per item (bits 0-7), whether the item's
 // geometry is staged in shared memory (bit 8), the byte size of the force
-// scratch that precedes the staged geometry, in 16-byte units (bits 9-23), and
-// whether the force scratch lives in global memory instead (bit 24).
+// scratch that precedes the staged geometry, in 16-byte units (bits 9-23),
+// whether the force scratch lives in global memory instead (bit 24), and log2 of
+// the G of the configuration's default-rule tile (bits 25-27), whose summation
+// order every tile of a force item reproduces.
 __host__ __device__ __forceinline__ int item_G(const WorkItem& it) { return it.G & 0xff; }
 __host__ __device__ __forceinline__ bool item_staged(const WorkItem& it) { return (it.G >> 8) & 1; }
 __host__ __device__ __forceinline__ size_t item_fbytes(const WorkItem& it) { return (size_t)((it.G >> 9) & 0x7fff) * 16; }
 __host__ __device__ __forceinline__ bool item_global(const WorkItem& it) { return (it.G >> 24) & 1; }
-__host__ __device__ __forceinline__ int pack_G(int G, bool staged, size_t fbytes, bool global = false) {
-  return G | (staged ? 1 << 8 : 0) | (int)(((fbytes + 15) / 16) << 9) | (global ? 1 << 24 : 0);
+__host__ __device__ __forceinline__ int item_Grule(const WorkItem& it) { return 1 << ((it.G >> 25) & 7); }
+__host__ __device__ __forceinline__ int pack_G(int G, bool staged, size_t fbytes, bool global = false, int Grule = 0) {
+  int lg = 0;
+  while ((1 << lg) < (Grule ? Grule : G)) ++lg;
+  return G | (staged ? 1 << 8 : 0) | (int)(((fbytes + 15) / 16) << 9) | (global ? 1 << 24 : 0) | (lg << 25);
 }
 
 // Fixed-order fold of per-lane partial sums held in shared memory as
@@ -546,12 +551,11 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
 // ST: staged (1) or in-place CSR (0) geometry, or decided per item (-1).
 // Bytes of the force items' shared-memory table of per-individual constants (G entries).
 __host__ __device__ constexpr size_t tersoff_table_bytes(int G) { return ((size_t)G * sizeof(TersoffC) + 15) & ~(size_t)15; }
-// The per-(individual, atom) squared force errors of a force item: row g holds the item's atoms
-// in chunks of 32, each chunk padded by one double (consecutive chunks start in different banks).
-// Shared-memory items keep them in the f_ij scratch once every f_ij has been read; an item with
-// its scratch in global memory keeps them after it.
-__host__ __device__ constexpr int ferr_row(int Na) { return Na + ((Na + 31) >> 5); }
-__host__ __device__ constexpr int ferr_pos(int il) { return il + (il >> 5); }
+// A force item whose G differs from its configuration's default-rule G keeps the
+// per-(individual, atom) squared force errors in a table, row g = the item's atoms: shared-memory
+// items in the f_ij scratch once every f_ij has been read, an item with its scratch in global
+// memory after it.
+__host__ __device__ constexpr int ferr_row(int Na) { return Na; }
 // Atoms per thread in a shared-memory force item's gather pass, at most: their squared errors
 // wait in registers until the scratch is free.  The host's G rule keeps Na * G <= 256 * this.
 __host__ __device__ constexpr int ferr_steps(int zc) { return zc == 4 ? 6 : (zc == 8 ? 4 : 2); }
@@ -636,7 +640,7 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
   }
   __syncthreads();
   const int N = S.N, Nf = S.N_force;
-  const int nq = (Na + 31) >> 5, NaP = ferr_row(Na);
+  const int Gr = item_Grule(it);
   // gather pass: F_i = sum_j (f_ij - f_ji) of (individual g, atom il) and its squared error
   auto atom_error = [&](int il) -> double {
     const int i = atom0 + il;
@@ -664,31 +668,46 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
     }
     return dx * dx + dy * dy + dz * dz;
   };
-  // Canonical sum of each individual's squared force errors: every chunk of 32 consecutive atoms
-  // summed in atom order by one thread (tasks = G * nq <= BLK for shared-memory items), the
-  // chunk sum stored over the chunk's first entry, then the chunk sums in atom order.  The result
-  // depends on neither G, nor the block shape, nor the staging, so every force-item tiling gives
-  // the same bits.
-  auto fold = [&](double* ftab) {
-    for (int t = threadIdx.x; t < G * nq; t += BLK) {
-      const int gg = t / nq, q = t - gg * nq;
-      double* row = ftab + gg * NaP + 33 * q;
-      const int m = min(32, Na - 32 * q);
-      double acc = 0.0;
-#pragma unroll 4
-      for (int k = 0; k < m; ++k) acc += row[k];
-      row[0] = acc;
+  // Each individual's squared force errors are summed in the order of the configuration's
+  // default-rule tile (Gr individuals per item, Ar = 32 / Gr atoms per warp step, 8 warps): per
+  // thread the atoms w Ar + a + 8 Ar k in k order, then the 8 warps' sums in warp order
+  // (fold_item), then a butterfly over the Ar atom slots (a pairwise tree in slot order: each
+  // step adds two partners' values, and a + b == b + a).  An item of that tile sums in that
+  // order as it goes; any other tile (another G, or 32 individuals with global scratch) keeps the
+  // errors in a table and one warp per Gr individuals replays the order.  Every tile therefore
+  // gives the same bits, and the default tile pays nothing for it.
+  if (G == Gr) {
+    double ferr = 0.0;
+    for (int base = warp * A; base < Na; base += NW * A) {
+      const int il = base + aslot;
+      if (il < Na) ferr += atom_error(il);
     }
-    __syncthreads();
-    for (int gg = threadIdx.x; gg < G; gg += BLK) {
-      double acc = 0.0;
-      for (int q = 0; q < nq; ++q) acc += ftab[gg * NaP + 33 * q];
+    __syncthreads();  // the fold overwrites the f_ij scratch
+#pragma unroll
+    for (int k = 0; k < 7; ++k) red[k * BLK + threadIdx.x] = 0.0;
+    red[7 * BLK + threadIdx.x] = ferr;
+    fold_item<GT>(it, P, S.Nc, red, res);
+    return;
+  }
+  auto replay = [&](const double* ftab) {
+    const int Ar = 32 / Gr, gr = lane & (Gr - 1), a = lane / Gr;
+    for (int gb = warp * Gr; gb < G; gb += NW * Gr) {  // warp-uniform: every lane takes the shuffles
+      const int gg = gb + gr;
+      double s = 0.0;
+      if (gg < G) {
+        for (int w = 0; w < NW; ++w) {
+          double t = 0.0;
+          for (int il = w * Ar + a; il < Na; il += NW * Ar) t += ftab[(size_t)gg * Na + il];
+          s += t;
+        }
+      }
+      for (int o = Gr; o < 32; o <<= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
       const int pp = it.p0 + gg;
-      if (pp < P) {
+      if (a == 0 && gg < G && pp < P) {
         double* r = res + ((size_t)pp * S.Nc + c) * kResK;
 #pragma unroll
         for (int k = 0; k < 7; ++k) r[k] = 0.0;
-        r[7] = acc;
+        r[7] = s;
       }
     }
   };
@@ -696,10 +715,10 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
     double* ftab = reinterpret_cast<double*>(fsm + (size_t)ZC * Na * 3 * 32);
     for (int base = warp * A; base < Na; base += NW * A) {
       const int il = base + aslot;
-      if (il < Na) ftab[g * NaP + ferr_pos(il)] = atom_error(il);
+      if (il < Na) ftab[(size_t)g * Na + il] = atom_error(il);
     }
     __syncthreads();
-    fold(ftab);
+    replay(ftab);
   } else {
     // the errors wait in registers (at most ferr_steps per thread, by the host's G rule) until
     // every f_ij has been read, then take the scratch's place
@@ -720,10 +739,10 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
 #pragma unroll
     for (int k = 0; k < KS; ++k) {
       const int il = (warp + k * NW) * A + aslot;
-      if (il < Na) ftab[g * NaP + ferr_pos(il)] = ev[k];
+      if (il < Na) ftab[g * Na + il] = ev[k];
     }
     __syncthreads();
-    fold(ftab);
+    replay(ftab);
   }
 }
 
@@ -1474,7 +1493,7 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
     const bool force = c < ts.Nc_force;
     const int Na = ts.Na[c];
     const int mode = (modes && !modes->empty() && (*modes)[c] > 0) ? (*modes)[c] : kTileDefault;
-    int zc = 0, G = 32;
+    int zc = 0, G = 32, Grule = 32;
     size_t smem = kRedBytes;
     bool staged = false, global = false;
     size_t fbytes = 0, item_floats = 0;
@@ -1500,20 +1519,24 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
       auto fits = [&](int g) {
         return scratch(g) <= force_smem_target(zc) && (size_t)Na * g <= (size_t)ferr_steps(zc) * kBlock;
       };
-      if (force && (!fits(1) || mode == kTileGlobal)) {
+      // default rule: the largest G whose scratch fits, and the geometry staged too when it fits
+      // beside the scratch of >= 4 individuals; 32 individuals with global scratch when not even
+      // one individual's scratch fits.  Its G fixes the summation order of every tile.
+      const bool rule_global = !fits(1);
+      if (force && !rule_global) {
+        while (Grule > 1 && !fits(Grule)) Grule >>= 1;
+        int Gs = Grule;
+        while (Gs > 4 && scratch(Gs) + stage > stage_target(zc)) Gs >>= 1;
+        if (scratch(Gs) + stage <= stage_target(zc)) Grule = Gs;
+      }
+      if (force && (rule_global || mode == kTileGlobal)) {
         // 32 individuals per item (lane = individual, one atom per warp step, coalesced scratch
-        // rows) with the scratch (ZC slots) and the squared-error table in global memory: the
-        // only tile when not even one individual's scratch fits shared memory
+        // rows) with the scratch (ZC slots) and the squared-error table in global memory
         global = true;
         item_floats = ((size_t)zc * Na * 3 * 32 + (size_t)2 * ferr_row(Na) * 32 + 63) & ~(size_t)63;
         smem = std::max(smem, kRedBytes + tersoff_table_bytes(32));
       } else if (force) {
-        // default rule: the largest G whose scratch fits, and the geometry staged too when it fits
-        // beside the scratch of >= 4 individuals
-        while (G > 1 && !fits(G)) G >>= 1;
-        int Gs = G;
-        while (Gs > 4 && scratch(Gs) + stage > stage_target(zc)) Gs >>= 1;
-        if (scratch(Gs) + stage <= stage_target(zc)) G = Gs;
+        G = Grule;
         if (mode == kTileHalf) G = std::max(1, G / 2);
         if (mode == kTileQuarter) G = std::max(1, G / 4);
         staged = mode != kTileUnstaged && scratch(G) + stage <= stage_target(zc);
@@ -1554,7 +1577,7 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
         *gscratch_floats += item_floats;
       }
       groups[key].push_back(
-          {WorkItem{c, p0, pack_G(G, staged, fbytes, global), job, gofs}, cf * cnt, (double)Na * cnt, cf * cnt, cs * cnt});
+          {WorkItem{c, p0, pack_G(G, staged, fbytes, global, Grule), job, gofs}, cf * cnt, (double)Na * cnt, cf * cnt, cs * cnt});
     }
   }
   return GPUGA_OK;
