@@ -65,6 +65,8 @@ def parse_args():
     ap.add_argument("--no-serving", action="store_true", help="skip the bounded serving block")
     ap.add_argument("--tiles", type=int, default=0, choices=range(6),
                     help="Tersoff force-item tiles: 0 autotune (default), 1-5 one tile for every configuration")
+    ap.add_argument("--fitness-fold", type=int, default=0, choices=range(3),
+                    help="fitness fold: 0 by launch-set size (default), 1 in the work items, 2 in its own launch")
     ap.add_argument("--ga-generations", type=int, default=20,
                     help="generations of the full GA loop timed on the host and on the device loop (0 = skip)")
     return ap.parse_args()
@@ -239,12 +241,15 @@ def oracle_evaluator():
 
 
 TILES = 0  # force-item tiles of the batched Tersoff path (0: autotuned per configuration size)
+FOLD = 0   # where the fitness is folded (0: by the launch set's size, 1 in the work items, 2 own launch)
 
 
 def engine_opts(data, device):
     kw = dict(device=device)
     if TILES:
         kw.update(tiles=TILES)
+    if FOLD:
+        kw.update(fitness_fold=FOLD)
     if int(data["potential_type"]) == 3:
         kw.update(nn2b_r1=float(data["nn2b_r1"]), nn2b_r2=float(data["nn2b_r2"]))
     return kw
@@ -290,7 +295,9 @@ def run_ours(args, dist: Dist):
     n_launch = C.c_int()
     _lib.check(L.gpuga_plan_info(h, P, C.byref(n_launch), None, 0))
     tiles = tile_summary(e, data, P)
-    kernels_per_step = n_launch.value + 2  # + decode + fitness fold
+    n_kernels = C.c_int()
+    _lib.check(L.gpuga_plan_kernels(h, P, C.byref(n_kernels)))
+    kernels_per_step = n_kernels.value  # decode + item launches (+ the fitness fold's own launch)
 
     # ---- value: device-resident inputs, device time per step, L2 flushed between steps
     for k in range(nwarm):
@@ -329,7 +336,8 @@ def run_ours(args, dist: Dist):
     kinds = {0: "tersoff_batched", 1: "pair_batched<RI>", 2: "pair_batched<NN2B>"}
     launches = []
     for r in rows:
-        launches.append({"kernel": f"{kinds[int(r[0])]}<{int(r[1])},{'force' if r[2] else 'energy_virial'}>",
+        items = {0: "energy_virial", 1: "force", 2: "force+energy_virial"}[int(r[2])]
+        launches.append({"kernel": f"{kinds[int(r[0])]}<{int(r[1])},{items}>",
                          "ctas": int(r[3]), "units": r[4], "flops": r[5], "sfu_calls": r[6], "ms": r[7],
                          "tflops": (r[5] / (r[7] * 1e-3) / 1e12) if r[7] > 0 else None})
     dom = max(launches, key=lambda x: x["ms"])
@@ -603,9 +611,9 @@ def run_serving(args, steady: bool = False) -> dict:
 
 
 def main():
-    global TILES
+    global TILES, FOLD
     args = parse_args()
-    TILES = args.tiles
+    TILES, FOLD = args.tiles, args.fitness_fold
     if args.serving:
         print(json.dumps(run_serving(args)))
         return 0

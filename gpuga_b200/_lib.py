@@ -32,7 +32,7 @@ class GpugaError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("device", C.c_int), ("path", C.c_int), ("use_graph", C.c_int), ("nn2b_consistent", C.c_int),
                 ("nn2b_r1", C.c_float), ("nn2b_r2", C.c_float), ("verbose", C.c_int), ("neighbor_cells", C.c_int),
-                ("ri_self_energy", C.c_int), ("tiles", C.c_int)]
+                ("ri_self_energy", C.c_int), ("tiles", C.c_int), ("fitness_fold", C.c_int)]
 
 
 FITNESS_CB = C.CFUNCTYPE(None, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_void_p)
@@ -58,6 +58,7 @@ PROTOTYPES = {
     "gpuga_last_config_results": (i32, [vp, i32, vp, vp, vp]),
     "gpuga_batched_forces": (i32, [vp, i32, vp, vp]),
     "gpuga_plan_info": (i32, [vp, i32, vp, vp, i32]),
+    "gpuga_plan_kernels": (i32, [vp, i32, vp]),
     "gpuga_kernel_timing": (i32, [vp, i32, i32]),
     "gpuga_calibrate_fp32": (i32, [i32, vp]),
     "gpuga_find_force64": (i32, [vp, vp, vp, vp, vp]),

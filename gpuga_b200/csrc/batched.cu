@@ -228,18 +228,21 @@ __device__ __forceinline__ void cutoff_fn(float r1, float r2, float pf, float d,
 // WorkItem::G packs the individuals per item (bits 0-7), whether the item's
 // geometry is staged in shared memory (bit 8), the byte size of the force
 // scratch that precedes the staged geometry, in 16-byte units (bits 9-23),
-// whether the force scratch lives in global memory instead (bit 24), and log2 of
+// whether the force scratch lives in global memory instead (bit 24), log2 of
 // the G of the configuration's default-rule tile (bits 25-27), whose summation
-// order every tile of a force item reproduces.
+// order every tile of a force item reproduces, and whether the item is a force
+// item (bit 28; energy/virial items otherwise).
 __host__ __device__ __forceinline__ int item_G(const WorkItem& it) { return it.G & 0xff; }
 __host__ __device__ __forceinline__ bool item_staged(const WorkItem& it) { return (it.G >> 8) & 1; }
 __host__ __device__ __forceinline__ size_t item_fbytes(const WorkItem& it) { return (size_t)((it.G >> 9) & 0x7fff) * 16; }
 __host__ __device__ __forceinline__ bool item_global(const WorkItem& it) { return (it.G >> 24) & 1; }
 __host__ __device__ __forceinline__ int item_Grule(const WorkItem& it) { return 1 << ((it.G >> 25) & 7); }
-__host__ __device__ __forceinline__ int pack_G(int G, bool staged, size_t fbytes, bool global = false, int Grule = 0) {
+__host__ __device__ __forceinline__ bool item_force(const WorkItem& it) { return (it.G >> 28) & 1; }
+__host__ __device__ __forceinline__ int pack_G(int G, bool staged, size_t fbytes, bool global, int Grule, bool force) {
   int lg = 0;
   while ((1 << lg) < (Grule ? Grule : G)) ++lg;
-  return G | (staged ? 1 << 8 : 0) | (int)(((fbytes + 15) / 16) << 9) | (global ? 1 << 24 : 0) | (lg << 25);
+  return G | (staged ? 1 << 8 : 0) | (int)(((fbytes + 15) / 16) << 9) | (global ? 1 << 24 : 0) | (lg << 25) |
+         (force ? 1 << 28 : 0);
 }
 
 // Fixed-order fold of per-lane partial sums held in shared memory as
@@ -746,24 +749,100 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
   }
 }
 
+// fitness.cu:329-331, 437-555 in FP64 for individual p, by one warp: lane c sums configurations
+// c, c + 32, ... in order, then a butterfly; the same order whichever warp or launch folds.
+// Reads go through L2 (ld.cg): other CTAs of the same launch wrote the results.
+__device__ __forceinline__ void fold_fitness(const JobView& J, int p, int lane) {
+  const int Nc = J.v.Nc, Nc_force = J.Nc_force;
+  const double* __restrict__ res = J.res;
+  const double* __restrict__ E_ref = J.E_ref;
+  const double* __restrict__ W_ref = J.W_ref;
+  double eE = 0, eW = 0, eF = 0;
+  for (int c = lane; c < Nc; c += 32) {
+    const double* r = res + ((size_t)p * Nc + c) * kResK;
+    if (c >= Nc_force) {
+      const double de = __ldcg(r) - E_ref[c];
+      eE += de * de;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double dw = __ldcg(r + 1 + k) - W_ref[c + (size_t)Nc * k];
+        eW += dw * dw;
+      }
+    } else {
+      eF += __ldcg(r + 7);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    eE += __shfl_xor_sync(0xffffffffu, eE, o);
+    eW += __shfl_xor_sync(0xffffffffu, eW, o);
+    eF += __shfl_xor_sync(0xffffffffu, eF, o);
+  }
+  if (lane == 0) {
+    const double rE = sqrt(eE / J.nE), rW = sqrt(eW / J.nW), rF = sqrt(eF / J.nF);
+    J.fitness[p] = (double)J.wE * rE + (double)J.wW * rW + (double)J.wF * rF;
+    if (J.comps) {
+      J.comps[3 * (size_t)p + 0] = rE;
+      J.comps[3 * (size_t)p + 1] = rW;
+      J.comps[3 * (size_t)p + 2] = rF;
+    }
+  }
+}
+
+// End of every work item: its results for individuals p0 .. p0 + G - 1 are written.  Each of those
+// individuals' completion count goes up by one with a release-acquire atomic (the CTA barrier
+// orders every thread's writes before it, and release is cumulative); the item that brings an individual to Nc
+// configurations folds its fitness and resets the count for the next generation.  Nothing waits.
+// Release-acquire increment at device scope: releases the CTA's writes ordered before it (by the
+// preceding CTA barrier) and acquires the writes released by earlier increments.
+__device__ __forceinline__ int atomic_add_acq_rel(int* a, int v) {
+  int old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(a), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void finish_item(const JobView* __restrict__ jobs, const WorkItem& it, int G) {
+  const JobView& J = jobs[it.job];
+  if (!J.fit_count) return;
+  __shared__ int s_last[32];
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int p = it.p0 + threadIdx.x;
+    int last = 0;
+    if (threadIdx.x < G && p < J.P) last = atomic_add_acq_rel(&J.fit_count[p], 1) == J.v.Nc - 1;
+    s_last[threadIdx.x] = last;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int g = threadIdx.x >> 5; g < G; g += blockDim.x >> 5) {
+    if (!s_last[g]) continue;  // warp-uniform
+    __threadfence();
+    fold_fitness(J, it.p0 + g, lane);
+    if (lane == 0) J.fit_count[it.p0 + g] = 0;
+  }
+}
+
 // Energy/virial Tersoff items read their geometry through L1: staging it in shared memory
 // would cap the CTAs per SM without making the per-atom loads cheaper (measured).
 constexpr bool kStageEV = false;
 
-// LO: the job's derived constants need their FP64 remainders (tersoff_consts_exact).
-template <int ZC, int NT, bool FORCE, int BLK, bool LO>
-__global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_batched(const JobView* __restrict__ jobs,
-                                                       const WorkItem* __restrict__ items) {
+// LO: the job's derived constants need their FP64 remainders (tersoff_consts_exact).  One launch
+// holds both kinds of items (item_force), 256 threads each: three CTAs per SM for ZC = 4 bound
+// both bodies to 80 registers (the energy/virial body measured as fast there as in 128-thread
+// CTAs at 96 registers, five per SM).
+template <int ZC, int NT, bool LO>
+__global__ void __launch_bounds__(kBlock, ZC == 4 ? 3 : 1) tersoff_batched(const JobView* __restrict__ jobs,
+                                                                          const WorkItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem[];
   const WorkItem it = items[blockIdx.x];
-  if constexpr (!FORCE) {
+  if (!item_force(it)) {
     // energy/virial items: always 32 individuals (the run-time geometry form: the CSR-only
     // specialisation spilled at this kernel's register bound and ran 5 % slower)
-    tersoff_item<ZC, NT, FORCE, BLK, 32, -1, LO>(jobs, it, smem);
+    tersoff_item<ZC, NT, false, kBlock, 32, -1, LO>(jobs, it, smem);
   } else if constexpr (ZC == 4) {
 #define GPUGA_TI(GG)                                    \
   case GG:                                              \
-    tersoff_item<ZC, NT, FORCE, BLK, GG, 1, LO>(jobs, it, smem); \
+    tersoff_item<ZC, NT, true, kBlock, GG, 1, LO>(jobs, it, smem); \
     break;
     switch (item_G(it)) {
       GPUGA_TI(32)
@@ -775,8 +854,9 @@ __global__ void __launch_bounds__(BLK, ZC == 4 ? (FORCE ? 3 : 5) : 1) tersoff_ba
     }
 #undef GPUGA_TI
   } else {
-    tersoff_item<ZC, NT, FORCE, BLK, 0, -1, LO>(jobs, it, smem);
+    tersoff_item<ZC, NT, true, kBlock, 0, -1, LO>(jobs, it, smem);
   }
+  finish_item(jobs, it, item_G(it));
 }
 
 // --------------------------------------------------------------------------- RI / NN2B
@@ -996,13 +1076,8 @@ __device__ __forceinline__ void nn_pairs(const float* __restrict__ wsm, int lane
   for (int u = 0; u < NP; ++u) p2[u] = with_p2 ? (float)(p2d[u] - (double)b2) : 0.f;
 }
 
-// RI: three CTAs per SM (at most 85 registers); NN2B: two (128 registers, two pairs per
-// weight load) -- each measured faster than the unbounded register allocation.
 template <int KIND, int NMAX, bool FORCE>
-__global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const JobView* __restrict__ jobs,
-                                                       const WorkItem* __restrict__ items) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const WorkItem it = items[blockIdx.x];
+__device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, const WorkItem& it, unsigned char* smem) {
   const JobView& J = jobs[it.job];
   const DevView S = J.v;
   const int P = J.P, Pstride = J.Pstride, nn = J.num_neurons, nv = J.num_vars;
@@ -1231,53 +1306,29 @@ __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const 
   reduce_item<32>(it, P, S.Nc, acc, smem, res);  // pair items hold 32 individuals
 }
 
+// RI: three CTAs per SM (at most 85 registers); NN2B: two (128 registers, two pairs per weight
+// load) -- each measured faster than the unbounded register allocation, and than NN2B at three
+// CTAs per SM (with either one or two pairs per weight load).  One launch holds both kinds of items.
+template <int KIND, int NMAX>
+__global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const JobView* __restrict__ jobs,
+                                                                         const WorkItem* __restrict__ items) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const WorkItem it = items[blockIdx.x];
+  if (item_force(it))
+    pair_item<KIND, NMAX, true>(jobs, it, smem);
+  else
+    pair_item<KIND, NMAX, false>(jobs, it, smem);
+  finish_item(jobs, it, 32);
+}
+
 // --------------------------------------------------------------------------- fitness
-// fitness.cu:329-331, 437-555 in FP64: one warp per individual of every job,
-// fixed-order sums.
+// The fitness of every individual in a launch of its own: for launch sets that compute only part
+// of the configurations' results (full sets fold in their work items, finish_item).
 __global__ void fitness_jobs(const JobView* __restrict__ jobs, const int2* __restrict__ indmap, int total) {
   const int t = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
   if (t >= total) return;
   const int2 jp = indmap[t];
-  const JobView& J = jobs[jp.x];
-  const int p = jp.y, Nc = J.v.Nc, Nc_force = J.Nc_force;
-  const double* __restrict__ res = J.res;
-  const double* __restrict__ E_ref = J.E_ref;
-  const double* __restrict__ W_ref = J.W_ref;
-  const double nF = J.nF, nE = J.nE, nW = J.nW;
-  const float wF = J.wF, wE = J.wE, wW = J.wW;
-  double* __restrict__ fitness = J.fitness;
-  double* __restrict__ comps = J.comps;
-  double eE = 0, eW = 0, eF = 0;
-  for (int c = lane; c < Nc; c += 32) {
-    const double* r = res + ((size_t)p * Nc + c) * kResK;
-    if (c >= Nc_force) {
-      const double de = r[0] - E_ref[c];
-      eE += de * de;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        const double dw = r[1 + k] - W_ref[c + (size_t)Nc * k];
-        eW += dw * dw;
-      }
-    } else {
-      eF += r[7];
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    eE += __shfl_xor_sync(0xffffffffu, eE, o);
-    eW += __shfl_xor_sync(0xffffffffu, eW, o);
-    eF += __shfl_xor_sync(0xffffffffu, eF, o);
-  }
-  if (lane == 0) {
-    const double rE = sqrt(eE / nE), rW = sqrt(eW / nW), rF = sqrt(eF / nF);
-    fitness[p] = (double)wE * rE + (double)wW * rW + (double)wF * rF;
-    if (comps) {
-      comps[3 * (size_t)p + 0] = rE;
-      comps[3 * (size_t)p + 1] = rW;
-      comps[3 * (size_t)p + 2] = rF;
-    }
-  }
+  fold_fitness(jobs[jp.x], jp.y, threadIdx.x & 31);
 }
 
 // --------------------------------------------------------------------------- planning
@@ -1288,10 +1339,11 @@ constexpr size_t kRedBytes = (size_t)kWarps * 32 * kResK * sizeof(double);
 // (measured).  Larger register classes would spill under that bound and keep two CTAs per SM.
 size_t force_smem_target(int zc) { return zc == 4 ? 72 * 1024 : 96 * 1024; }
 size_t stage_target(int zc) { return zc == 4 ? 74 * 1024 : 110 * 1024; }  // force scratch + staged geometry
-// Energy/virial Tersoff items run in 128-thread CTAs (more resident warps per SM at ~115
-// registers per thread); kStageEV (above) keeps their geometry in place.
-constexpr int kBlockEV = 128;
 constexpr size_t kSmemMax = 220 * 1024;
+// gpuga_options.fitness_fold = 0: launch sets of at most this many work items fold the fitness in
+// their items (measured on B200: 290 items, 0.073 -> 0.067 ms per generation), larger ones in a
+// launch of its own (62 170 items: 4.79 -> 4.63 ms; the count's round trip holds every CTA's slot).
+constexpr size_t kFoldInItemsMax = 4096;
 
 int zclass_of(int z) { return tersoff_zclass(z); }
 }  // namespace
@@ -1375,6 +1427,7 @@ JobView make_job_view(const Engine* e, const Plan* plan) {
   j.wW = d.w_stress;
   j.fitness = plan->d_fitness;
   j.comps = plan->d_comps;
+  j.fit_count = plan->d_fitcnt;
   return j;
 }
 
@@ -1544,8 +1597,8 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
         smem = std::max(smem, scratch(G) + (staged ? stage : 0));
       } else {
         // energy/virial items (always G = 32, which tersoff_batched compiles in): per-lane FP64
-        // sums of the 128-thread CTA, then (optionally) the geometry
-        smem = (size_t)kBlockEV * kResK * sizeof(double);
+        // sums of the 256-thread CTA, then (optionally; kStageEV) the geometry
+        smem = (size_t)kBlock * kResK * sizeof(double);
         if (kStageEV && stage <= stage_target(zc)) {
           staged = true;
           smem += stage;
@@ -1556,7 +1609,7 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
     } else {
       smem += kPairStageBytes;  // RI: the warps' two-stage pair buffers
     }
-    const LaunchKey key{kind, zc, nmax, force ? 1 : 0, lo ? 1 : 0};
+    const LaunchKey key{kind, zc, nmax, 0, lo ? 1 : 0};  // force and energy/virial items share launches
     smem_need[key] = std::max(smem_need[key], smem);
     double cf = 0, cs = 0;
     const bool half = kind != 0 && !force;
@@ -1577,7 +1630,7 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
         *gscratch_floats += item_floats;
       }
       groups[key].push_back(
-          {WorkItem{c, p0, pack_G(G, staged, fbytes, global, Grule), job, gofs}, cf * cnt, (double)Na * cnt, cf * cnt, cs * cnt});
+          {WorkItem{c, p0, pack_G(G, staged, fbytes, global, Grule, force), job, gofs}, cf * cnt, (double)Na * cnt, cf * cnt, cs * cnt});
     }
   }
   return GPUGA_OK;
@@ -1594,49 +1647,44 @@ int set_smem(K kernel) {
 int launch_one(const LaunchSet* ls, const Launch& L, cudaStream_t st, bool configure_only) {
   const dim3 grid(L.count), block(kBlock);
   const WorkItem* items = ls->d_items + L.first;
-#define GPUGA_TERSOFF1(ZC, NT, F)                                                       \
+#define GPUGA_TERSOFF1(ZC, NT)                                                          \
   do {                                                                                  \
-    constexpr int BLK = F ? kBlock : kBlockEV;                                          \
     if (configure_only) {                                                               \
-      if (L.lo) GPUGA_TRY(set_smem(tersoff_batched<ZC, NT, F, BLK, true>));             \
-      else GPUGA_TRY(set_smem(tersoff_batched<ZC, NT, F, BLK, false>));                 \
+      if (L.lo) GPUGA_TRY(set_smem(tersoff_batched<ZC, NT, true>));                     \
+      else GPUGA_TRY(set_smem(tersoff_batched<ZC, NT, false>));                         \
       break;                                                                            \
     }                                                                                   \
     if (L.lo)                                                                           \
-      tersoff_batched<ZC, NT, F, BLK, true><<<grid, dim3(BLK), L.smem, st>>>(ls->d_jobs, items); \
+      tersoff_batched<ZC, NT, true><<<grid, block, L.smem, st>>>(ls->d_jobs, items);     \
     else                                                                                \
-      tersoff_batched<ZC, NT, F, BLK, false><<<grid, dim3(BLK), L.smem, st>>>(ls->d_jobs, items); \
+      tersoff_batched<ZC, NT, false><<<grid, block, L.smem, st>>>(ls->d_jobs, items);    \
   } while (0)
-#define GPUGA_TERSOFF(ZC, F)                                                          \
+#define GPUGA_TERSOFF(ZC)                                                             \
   do {                                                                                \
-    if (L.nmax == 2) GPUGA_TERSOFF1(ZC, 2, F); else GPUGA_TERSOFF1(ZC, 1, F);         \
+    if (L.nmax == 2) GPUGA_TERSOFF1(ZC, 2); else GPUGA_TERSOFF1(ZC, 1);               \
   } while (0)
-#define GPUGA_PAIR(KD, NM, F)                                                         \
+#define GPUGA_PAIR(KD, NM)                                                            \
   do {                                                                                \
     if (configure_only) {                                                             \
-      GPUGA_TRY(set_smem(pair_batched<KD, NM, F>));                                   \
+      GPUGA_TRY(set_smem(pair_batched<KD, NM>));                                      \
       break;                                                                          \
     }                                                                                 \
-    pair_batched<KD, NM, F><<<grid, block, L.smem, st>>>(ls->d_jobs, items);          \
+    pair_batched<KD, NM><<<grid, block, L.smem, st>>>(ls->d_jobs, items);             \
   } while (0)
   if (L.kind == 0) {
-    if (L.zclass == 4) {
-      if (L.force) GPUGA_TERSOFF(4, true); else GPUGA_TERSOFF(4, false);
-    } else if (L.zclass == 8) {
-      if (L.force) GPUGA_TERSOFF(8, true); else GPUGA_TERSOFF(8, false);
-    } else {
-      if (L.force) GPUGA_TERSOFF(16, true); else GPUGA_TERSOFF(16, false);
-    }
+    if (L.zclass == 4) GPUGA_TERSOFF(4);
+    else if (L.zclass == 8) GPUGA_TERSOFF(8);
+    else GPUGA_TERSOFF(16);
   } else if (L.kind == 1) {
-    if (L.force) GPUGA_PAIR(1, 8, true); else GPUGA_PAIR(1, 8, false);
+    GPUGA_PAIR(1, 8);
   } else if (L.nmax == 8) {
-    if (L.force) GPUGA_PAIR(2, 8, true); else GPUGA_PAIR(2, 8, false);
+    GPUGA_PAIR(2, 8);
   } else if (L.nmax == 12) {
-    if (L.force) GPUGA_PAIR(2, 12, true); else GPUGA_PAIR(2, 12, false);
+    GPUGA_PAIR(2, 12);
   } else if (L.nmax == 16) {
-    if (L.force) GPUGA_PAIR(2, 16, true); else GPUGA_PAIR(2, 16, false);
+    GPUGA_PAIR(2, 16);
   } else {
-    if (L.force) GPUGA_PAIR(2, 32, true); else GPUGA_PAIR(2, 32, false);
+    GPUGA_PAIR(2, 32);
   }
 #undef GPUGA_TERSOFF
 #undef GPUGA_TERSOFF1
@@ -1703,7 +1751,9 @@ int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSe
     L.zclass = kv.first.zclass;
     L.nmax = kv.first.nmax;
     L.lo = kv.first.lo != 0;
-    L.force = kv.first.force != 0;
+    int nforce = 0;
+    for (auto& t : v) nforce += item_force(t.w) ? 1 : 0;
+    L.force = nforce == 0 ? 0 : (nforce == (int)v.size() ? 1 : 2);
     L.smem = smem_need[kv.first];
     L.count = (int)v.size();
     L.first = all.size();
@@ -1719,6 +1769,11 @@ int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSe
   std::stable_sort(ls->launches.begin(), ls->launches.end(),
                    [](const Launch& a, const Launch& b) { return a.flops > b.flops; });
   ls->total_individuals = (int)indmap.size();
+  // where the fitness is folded (gpuga_options.fitness_fold; a partial set never folds in its items)
+  const int fold_opt = jobs.empty() ? 2 : jobs[0].first->opt.fitness_fold;
+  ls->folds = !only && (fold_opt == 1 || (fold_opt == 0 && all.size() <= kFoldInItemsMax));
+  if (!ls->folds)
+    for (JobView& jv : ls->jobs) jv.fit_count = nullptr;
   GPUGA_CUDA(cudaMalloc(&ls->d_items, sizeof(WorkItem) * std::max<size_t>(all.size(), 1)));
   GPUGA_CUDA(cudaMemcpy(ls->d_items, all.data(), sizeof(WorkItem) * all.size(), cudaMemcpyHostToDevice));
   GPUGA_CUDA(cudaMalloc(&ls->d_indmap, sizeof(int2) * std::max<size_t>(indmap.size(), 1)));
@@ -1772,9 +1827,8 @@ int launchset_enqueue(LaunchSet* ls, cudaStream_t st) {
   const int total = ls->total_individuals;
   decode_jobs<<<(total + 127) / 128, 128, 0, st>>>(ls->d_jobs, ls->d_indmap, total);
   GPUGA_CUDA(cudaGetLastError());
-  bool any_side = false;
-  for (const Launch& L : ls->launches)
-    if (L.force && !ls->timing) any_side = true;
+  // several launches (job mixes with several kernel classes): every second one on the side stream
+  const bool any_side = ls->launches.size() > 1 && !ls->timing;
   if (any_side) {
     GPUGA_CUDA(cudaEventRecord(ls->fork, st));
     GPUGA_CUDA(cudaStreamWaitEvent(ls->side, ls->fork, 0));
@@ -1782,7 +1836,7 @@ int launchset_enqueue(LaunchSet* ls, cudaStream_t st) {
   GPUGA_TRY(launchset_collect_timing(ls));
   for (size_t k = 0; k < ls->launches.size(); ++k) {
     const Launch& L = ls->launches[k];
-    cudaStream_t s = L.force && any_side ? ls->side : st;
+    cudaStream_t s = (k & 1) && any_side ? ls->side : st;
     if (ls->timing) GPUGA_CUDA(cudaEventRecord(ls->tev[2 * k], s));
     GPUGA_TRY(launch_one(ls, L, s, false));
     if (ls->timing) GPUGA_CUDA(cudaEventRecord(ls->tev[2 * k + 1], s));
@@ -1792,8 +1846,10 @@ int launchset_enqueue(LaunchSet* ls, cudaStream_t st) {
     GPUGA_CUDA(cudaEventRecord(ls->join, ls->side));
     GPUGA_CUDA(cudaStreamWaitEvent(st, ls->join, 0));
   }
-  fitness_jobs<<<(total + 3) / 4, 128, 0, st>>>(ls->d_jobs, ls->d_indmap, total);
-  GPUGA_CUDA(cudaGetLastError());
+  if (!ls->folds) {  // a partial set: the fitness of every individual in one more launch
+    fitness_jobs<<<(total + 3) / 4, 128, 0, st>>>(ls->d_jobs, ls->d_indmap, total);
+    GPUGA_CUDA(cudaGetLastError());
+  }
   return GPUGA_OK;
 }
 
@@ -1885,6 +1941,8 @@ int plan_build(Engine* e, int P, Plan** out) {
   GPUGA_TRY(e->alloc(&plan->d_res, (size_t)P * d.Nc * kResK));
   GPUGA_TRY(e->alloc(&plan->d_fitness, (size_t)P));
   GPUGA_TRY(e->alloc(&plan->d_comps, (size_t)3 * P));
+  GPUGA_TRY(e->alloc(&plan->d_fitcnt, (size_t)P));
+  GPUGA_CUDA(cudaMemset(plan->d_fitcnt, 0, sizeof(int) * (size_t)P));
   GPUGA_TRY(e->alloc(&plan->d_pop, (size_t)P * d.num_vars));
   GPUGA_CUDA(cudaMallocHost(&plan->h_pop, sizeof(float) * (size_t)P * d.num_vars));
   GPUGA_CUDA(cudaMallocHost(&plan->h_fit, sizeof(double) * 4 * (size_t)P));
@@ -1904,6 +1962,10 @@ int plan_build(Engine* e, int P, Plan** out) {
     for (int c = 0; c < e->ts.Nc_force; ++c) plan->tiles[c] = (int8_t)tiles;
   } else if (tiles < 0 || tiles > kTileUnstaged) {
     set_error("gpuga_options.tiles must be 0..5 (got %d).", tiles);
+    return GPUGA_ERR_ARG;
+  }
+  if (e->opt.fitness_fold < 0 || e->opt.fitness_fold > 2) {
+    set_error("gpuga_options.fitness_fold must be 0..2 (got %d).", e->opt.fitness_fold);
     return GPUGA_ERR_ARG;
   }
   plan->ls.reset(new LaunchSet);

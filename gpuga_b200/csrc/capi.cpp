@@ -50,6 +50,7 @@ void gpuga_default_options(gpuga_options* opt) {
   opt->nn2b_r2 = 8.0f;
   opt->verbose = 0;
   opt->tiles = 0;
+  opt->fitness_fold = 0;
 }
 
 const char* gpuga_last_error(void) { return last_error(); }
@@ -266,7 +267,7 @@ int gpuga_plan_info(gpuga_engine* h, int P, int* n_launches, double* per_launch,
       double* o = per_launch + 8 * (size_t)k;
       o[0] = L.kind;
       o[1] = L.kind == 2 ? L.nmax : L.zclass;
-      o[2] = L.force ? 1 : 0;
+      o[2] = L.force;
       o[3] = L.count;
       o[4] = L.units;
       o[5] = L.flops;
@@ -274,6 +275,17 @@ int gpuga_plan_info(gpuga_engine* h, int P, int* n_launches, double* per_launch,
       o[7] = ls->t_count ? ls->t_ms[k] / ls->t_count : 0.0;
     }
   }
+  return GPUGA_OK;
+}
+
+int gpuga_plan_kernels(gpuga_engine* h, int P, int* kernels) {
+  CHECK_ARG(h && P > 0 && kernels, "gpuga_plan_kernels: invalid argument");
+  Plan* plan = nullptr;
+  GPUGA_CUDA(cudaSetDevice(h->e->device));
+  int s = plan_get(h->e, P, &plan);
+  if (s != GPUGA_OK) return s;
+  const LaunchSet* ls = plan->ls.get();
+  *kernels = 1 + (int)ls->launches.size() + (ls->folds ? 0 : 1);  // decode + items (+ fitness fold)
   return GPUGA_OK;
 }
 

@@ -154,13 +154,16 @@ struct JobView {
   float wF, wE, wW;
   double* fitness;       // [P]
   double* comps;         // [P][3]
+  int* fit_count;        // [P] configurations of this generation finished per individual; the work
+                         // item that finishes an individual's last one folds its fitness (reset to
+                         // 0 there).  Null: a partial launch set (no fold).
 };
 
 struct Launch {
   int kind = 0;        // 0 Tersoff, 1 RI, 2 NN2B
   int zclass = 4;      // Tersoff register-array size
   int nmax = 0;        // NN2B register-array size; Tersoff: number of atom types
-  bool force = false;  // force items (gather pass) vs energy/virial items
+  int force = 0;       // the launch's items: 0 energy/virial, 1 force (gather pass), 2 both
   bool lo = false;     // Tersoff: carry the FP64 remainders of the derived constants
   size_t smem = 0;
   int count = 0;
@@ -179,6 +182,7 @@ struct LaunchSet {
   WorkItem* d_items = nullptr;
   int2* d_indmap = nullptr;    // global individual -> (job, p)
   int total_individuals = 0;
+  bool folds = true;           // the items fold every individual's fitness (no fitness_jobs launch)
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   bool timing = false;               // event pair around every launch (eager launches)
@@ -214,6 +218,7 @@ struct Plan {
   double* d_res = nullptr;     // [P][Nc][kResK]
   double* d_fitness = nullptr; // [P]
   double* d_comps = nullptr;   // [P][3]
+  int* d_fitcnt = nullptr;     // [P] per-generation completion counts (JobView::fit_count)
   float* d_pop = nullptr;      // [P][d] staging
   float* h_pop = nullptr;      // pinned
   double* h_fit = nullptr;     // pinned [4P]: fitness + 3 components

@@ -22,7 +22,7 @@ def _p(a: np.ndarray):
 
 def options(device: int = 0, path: int = PATH_BATCHED, use_graph: bool = True, nn2b_consistent: bool = False,
             nn2b_r1: float = 7.0, nn2b_r2: float = 8.0, verbose: bool = False, neighbor_cells: int = 0,
-            ri_self_energy: bool = False, tiles: int = 0) -> _lib.Options:
+            ri_self_energy: bool = False, tiles: int = 0, fitness_fold: int = 0) -> _lib.Options:
     o = _lib.Options()
     _lib.load().gpuga_default_options(C.byref(o))
     o.device, o.path, o.use_graph = device, path, int(use_graph)
@@ -30,6 +30,7 @@ def options(device: int = 0, path: int = PATH_BATCHED, use_graph: bool = True, n
     o.neighbor_cells = neighbor_cells
     o.ri_self_energy = int(ri_self_energy)
     o.tiles = tiles
+    o.fitness_fold = fitness_fold
     return o
 
 

@@ -64,6 +64,12 @@ typedef struct gpuga_options {
                           count whose scratch fits shared memory), 2 half of it, 3 a quarter, 4 32
                           individuals with the scratch in global memory, 5 the fixed rule without staged
                           geometry.  Every choice gives bit-identical results. */
+  int fitness_fold;    /* where each individual's fitness is folded from its configurations' results:
+                          1 in the work item that finishes its last configuration (an atomic count per
+                          individual; one launch per generation besides the decode), 2 in a launch of its
+                          own after the items, 0 (default) 1 for launch sets of at most 4096 work items
+                          (launch-bound sizes), 2 above (the count's round trip at the end of every item
+                          costs more there than the extra launch). */
 } gpuga_options;
 
 /* Fills *opt with the reference's semantics (batched path, graphs on, NN2B taper 7..8 A, force quirk kept). */
@@ -135,15 +141,20 @@ int gpuga_last_config_results(gpuga_engine* e, int P, double* energy, double* vi
 int gpuga_batched_forces(gpuga_engine* e, int P, const float* pop01, float* forces_out);
 
 /* Launch plan of the batched path for population size P (built on first use).
- * *n_launches = batched force launches per generation (decode and fitness-fold launches come on top);
+ * *n_launches = batched launches per generation (one per kernel class: force and energy/virial items
+ * share a launch, and the items fold each individual's fitness; the decode launch comes on top);
  * per_launch (may be NULL) receives up to `cap` rows of 8 doubles:
- * {kind (0 Tersoff, 1 RI, 2 NN2B), register class, force items?, CTAs, (individual, atom) units,
- *  algorithmic FP32 flops, transcendental calls, mean device ms per generation while timing is on}. */
+ * {kind (0 Tersoff, 1 RI, 2 NN2B), register class, items (0 energy/virial, 1 force, 2 both), CTAs,
+ *  (individual, atom) units, algorithmic FP32 flops, transcendental calls, mean device ms per
+ *  generation while timing is on}. */
+int gpuga_plan_info(gpuga_engine* e, int P, int* n_launches, double* per_launch, int cap);
+/* Kernel launches per generation of the batched path for population size P: the decode, the item
+ * launches and, when the items do not fold the fitness (gpuga_options.fitness_fold), the fold. */
+int gpuga_plan_kernels(gpuga_engine* e, int P, int* kernels);
 /* The force-item tile of every configuration (tiles[Nc], gpuga_options.tiles codes 1-5; 0 for
  * energy/virial and non-Tersoff configurations) of the plan for population size P, and the host time
  * the autotuner spent on it. */
 int gpuga_plan_tiles(gpuga_engine* e, int P, int* tiles, int cap, double* tune_ms);
-int gpuga_plan_info(gpuga_engine* e, int P, int* n_launches, double* per_launch, int cap);
 /* Records CUDA events around every batched launch of population size P (eager launches only:
  * gpuga_fitness_device, or gpuga_fitness with use_graph = 0).  While timing is on, the launches
  * of a generation run one after another on the caller's stream, so each duration is that
