@@ -66,7 +66,7 @@ def parse_args():
     ap.add_argument("--tiles", type=int, default=0, choices=range(6),
                     help="Tersoff force-item tiles: 0 autotune (default), 1-5 one tile for every configuration")
     ap.add_argument("--fitness-fold", type=int, default=0, choices=range(3),
-                    help="fitness fold: 0 by launch-set size (default), 1 in the work items, 2 in its own launch")
+                    help="fitness fold: 0 (default) or 2 in its own launch, 1 in the work items")
     ap.add_argument("--ga-generations", type=int, default=20,
                     help="generations of the full GA loop timed on the host and on the device loop (0 = skip)")
     return ap.parse_args()
@@ -241,7 +241,7 @@ def oracle_evaluator():
 
 
 TILES = 0  # force-item tiles of the batched Tersoff path (0: autotuned per configuration size)
-FOLD = 0   # where the fitness is folded (0: by the launch set's size, 1 in the work items, 2 own launch)
+FOLD = 0   # where the fitness is folded (0/2: its own launch, 1: in the work items)
 
 
 def engine_opts(data, device):

@@ -750,7 +750,9 @@ __device__ __forceinline__ void tersoff_item(const JobView* __restrict__ jobs, c
 }
 
 // fitness.cu:329-331, 437-555 in FP64 for individual p, by one warp: lane c sums configurations
-// c, c + 32, ... in order, then a butterfly; the same order whichever warp or launch folds.
+// c, c + 32, ... in order, then a butterfly; the same order whichever warp or launch folds, and
+// the same operations: every product and sum is an explicit intrinsic, so that the compiler's
+// choice of contracting a * b + c into an FMA cannot differ between the kernels this is inlined in.
 // Reads go through L2 (ld.cg): other CTAs of the same launch wrote the results.
 __device__ __forceinline__ void fold_fitness(const JobView& J, int p, int lane) {
   const int Nc = J.v.Nc, Nc_force = J.Nc_force;
@@ -762,11 +764,11 @@ __device__ __forceinline__ void fold_fitness(const JobView& J, int p, int lane) 
     const double* r = res + ((size_t)p * Nc + c) * kResK;
     if (c >= Nc_force) {
       const double de = __ldcg(r) - E_ref[c];
-      eE += de * de;
+      eE = __fma_rn(de, de, eE);
 #pragma unroll
       for (int k = 0; k < 6; ++k) {
         const double dw = __ldcg(r + 1 + k) - W_ref[c + (size_t)Nc * k];
-        eW += dw * dw;
+        eW = __fma_rn(dw, dw, eW);
       }
     } else {
       eF += __ldcg(r + 7);
@@ -780,7 +782,8 @@ __device__ __forceinline__ void fold_fitness(const JobView& J, int p, int lane) 
   }
   if (lane == 0) {
     const double rE = sqrt(eE / J.nE), rW = sqrt(eW / J.nW), rF = sqrt(eF / J.nF);
-    J.fitness[p] = (double)J.wE * rE + (double)J.wW * rW + (double)J.wF * rF;
+    J.fitness[p] = __dadd_rn(__dadd_rn(__dmul_rn((double)J.wE, rE), __dmul_rn((double)J.wW, rW)),
+                             __dmul_rn((double)J.wF, rF));
     if (J.comps) {
       J.comps[3 * (size_t)p + 0] = rE;
       J.comps[3 * (size_t)p + 1] = rW;
@@ -1006,11 +1009,15 @@ struct NNSmem {
 // NP pairs of the same lane at once: every weight loaded from shared memory
 // feeds the NP pairs (the hidden-to-hidden loads, not the FMAs, bound a
 // single pair).  Each pair's arithmetic is the same sequence as for NP = 1.
-template <int NMAX, int NP, bool FULL>
+// NR: the network width as a compile-time constant (0: n at run time, with the padding columns
+// of the last float4 group evaluated on their zero weights); with it the row loop unrolls and the
+// padding columns drop out.
+template <int NMAX, int NP, int NR>
 __device__ __forceinline__ void nn_pairs(const float* __restrict__ wsm, int lane, int n, const float (&d)[NP],
                                          bool with_p2, float (&p2)[NP], float (&f2)[NP]) {
-  if (FULL) n = NMAX;  // every row present: the row loop unrolls completely
+  if (NR) n = NR;
   constexpr int Q = NMAX / 4;
+  constexpr int NC = NR ? NR : NMAX;  // columns evaluated
   const float4* W1 = reinterpret_cast<const float4*>(wsm);
   const float4* V = W1 + NMAX * Q * 32;
   const float b2 = wsm[(size_t)(NMAX * Q * 32 + 4 * Q * 32) * 4 + lane];
@@ -1024,8 +1031,12 @@ __device__ __forceinline__ void nn_pairs(const float* __restrict__ wsm, int lane
     for (int u = 0; u < NP; ++u)
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        x1[u][4 * q + c] = tanhf(w0c[c] * d[u] - b0c[c]);
-        y1[u][4 * q + c] = (1.0f - x1[u][4 * q + c] * x1[u][4 * q + c]) * w0c[c];
+        if (4 * q + c < NC) {
+          x1[u][4 * q + c] = tanhf(w0c[c] * d[u] - b0c[c]);
+          y1[u][4 * q + c] = (1.0f - x1[u][4 * q + c] * x1[u][4 * q + c]) * w0c[c];
+        } else {
+          x1[u][4 * q + c] = y1[u][4 * q + c] = 0.f;
+        }
       }
   }
   double p2d[NP];
@@ -1035,7 +1046,7 @@ __device__ __forceinline__ void nn_pairs(const float* __restrict__ wsm, int lane
     p2d[u] = 0.0;
   }
   const int qa_end = (n + 3) >> 2;
-#pragma unroll (FULL ? NMAX / 4 : 1)
+#pragma unroll (NR ? NMAX / 4 : 1)
   for (int qa = 0; qa < qa_end; ++qa) {
     const float4 b1 = V[(2 * Q + qa) * 32 + lane];
     const float4 w2 = V[(3 * Q + qa) * 32 + lane];
@@ -1050,17 +1061,15 @@ __device__ __forceinline__ void nn_pairs(const float* __restrict__ wsm, int lane
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
           const float4 w = W1[(a * Q + q) * 32 + lane];
+          const float wc[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-          for (int u = 0; u < NP; ++u) {
-            x2[u] = fmaf(w.x, x1[u][4 * q], x2[u]);
-            y2[u] = fmaf(w.x, y1[u][4 * q], y2[u]);
-            x2[u] = fmaf(w.y, x1[u][4 * q + 1], x2[u]);
-            y2[u] = fmaf(w.y, y1[u][4 * q + 1], y2[u]);
-            x2[u] = fmaf(w.z, x1[u][4 * q + 2], x2[u]);
-            y2[u] = fmaf(w.z, y1[u][4 * q + 2], y2[u]);
-            x2[u] = fmaf(w.w, x1[u][4 * q + 3], x2[u]);
-            y2[u] = fmaf(w.w, y1[u][4 * q + 3], y2[u]);
-          }
+          for (int u = 0; u < NP; ++u)
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+              if (4 * q + m < NC) {
+                x2[u] = fmaf(wc[m], x1[u][4 * q + m], x2[u]);
+                y2[u] = fmaf(wc[m], y1[u][4 * q + m], y2[u]);
+              }
         }
 #pragma unroll
         for (int u = 0; u < NP; ++u) {
@@ -1279,10 +1288,13 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
         bool need_p2 = !FORCE;
 #pragma unroll
         for (int u = 0; u < NP; ++u) need_p2 |= d[u] >= tp.r1;
+        // the class's full width, the reference's largest width (10), or any other at run time
         if (nn == NMAX)
-          nn_pairs<NMAX, NP, true>(wsm, lane, nn, d, need_p2, p2, f2raw);
+          nn_pairs<NMAX, NP, NMAX>(wsm, lane, nn, d, need_p2, p2, f2raw);
+        else if (NMAX == 12 && nn == 10)
+          nn_pairs<NMAX, NP, NMAX == 12 ? 10 : 0>(wsm, lane, nn, d, need_p2, p2, f2raw);
         else
-          nn_pairs<NMAX, NP, false>(wsm, lane, nn, d, need_p2, p2, f2raw);
+          nn_pairs<NMAX, NP, 0>(wsm, lane, nn, d, need_p2, p2, f2raw);
 #pragma unroll
         for (int u = 0; u < NP; ++u) {
           if (b + u < bend) {
@@ -1340,10 +1352,6 @@ constexpr size_t kRedBytes = (size_t)kWarps * 32 * kResK * sizeof(double);
 size_t force_smem_target(int zc) { return zc == 4 ? 72 * 1024 : 96 * 1024; }
 size_t stage_target(int zc) { return zc == 4 ? 74 * 1024 : 110 * 1024; }  // force scratch + staged geometry
 constexpr size_t kSmemMax = 220 * 1024;
-// gpuga_options.fitness_fold = 0: launch sets of at most this many work items fold the fitness in
-// their items (measured on B200: 290 items, 0.073 -> 0.067 ms per generation), larger ones in a
-// launch of its own (62 170 items: 4.79 -> 4.63 ms; the count's round trip holds every CTA's slot).
-constexpr size_t kFoldInItemsMax = 4096;
 
 int zclass_of(int z) { return tersoff_zclass(z); }
 }  // namespace
@@ -1769,9 +1777,12 @@ int launchset_build(const std::vector<std::pair<Engine*, Plan*>>& jobs, LaunchSe
   std::stable_sort(ls->launches.begin(), ls->launches.end(),
                    [](const Launch& a, const Launch& b) { return a.flops > b.flops; });
   ls->total_individuals = (int)indmap.size();
-  // where the fitness is folded (gpuga_options.fitness_fold; a partial set never folds in its items)
-  const int fold_opt = jobs.empty() ? 2 : jobs[0].first->opt.fitness_fold;
-  ls->folds = !only && (fold_opt == 1 || (fold_opt == 0 && all.size() <= kFoldInItemsMax));
+  // where the fitness is folded (gpuga_options.fitness_fold; a partial set never folds in its items).
+  // The fold launch is the default: the count's round trip at the end of every item holds the
+  // item's CTA slot, which measured slower than the extra launch at every size (B200: 62 170 items
+  // 4.79 vs 4.63 ms per generation, 290 items 0.069 vs 0.062 ms).
+  const int fold_opt = jobs.empty() ? 0 : jobs[0].first->opt.fitness_fold;
+  ls->folds = !only && fold_opt == 1;
   if (!ls->folds)
     for (JobView& jv : ls->jobs) jv.fit_count = nullptr;
   GPUGA_CUDA(cudaMalloc(&ls->d_items, sizeof(WorkItem) * std::max<size_t>(all.size(), 1)));

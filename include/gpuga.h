@@ -65,11 +65,11 @@ typedef struct gpuga_options {
                           individuals with the scratch in global memory, 5 the fixed rule without staged
                           geometry.  Every choice gives bit-identical results. */
   int fitness_fold;    /* where each individual's fitness is folded from its configurations' results:
-                          1 in the work item that finishes its last configuration (an atomic count per
-                          individual; one launch per generation besides the decode), 2 in a launch of its
-                          own after the items, 0 (default) 1 for launch sets of at most 4096 work items
-                          (launch-bound sizes), 2 above (the count's round trip at the end of every item
-                          costs more there than the extra launch). */
+                          0 (default) or 2 in a launch of its own after the item launches; 1 in the work
+                          item that finishes the individual's last configuration (an atomic count per
+                          individual, so that a generation is the decode launch plus the item launch;
+                          the count's round trip at the end of every item measured slower than the extra
+                          launch).  All choices give the same bits. */
 } gpuga_options;
 
 /* Fills *opt with the reference's semantics (batched path, graphs on, NN2B taper 7..8 A, force quirk kept). */

@@ -1,7 +1,6 @@
 """Where each individual's fitness is folded (gpuga_options.fitness_fold): in the work item that
 finishes the individual's last configuration (1: a per-individual atomic count, reset by the
-folding item for the next generation), in a launch of its own (2), or chosen by the launch set's
-size (0).  The fold is the same fixed-order FP64 sum in every case, so fitness values and
+folding item for the next generation) or in a launch of its own (2, and the default 0).  The fold is the same fixed-order FP64 sum in every case, so fitness values and
 components must be bit-identical -- generation after generation, which also checks that the counts
 return to zero.  Reference: fitness.cu:329-331, 392-555 (the reference folds on the host)."""
 import ctypes as C
@@ -46,8 +45,10 @@ def test_fold_placement_gives_the_same_bits(index):
             results[fold] = (got, _kernels(e, P))
     (ref, k1), (sep, k2), (auto, k0) = results[1], results[2], results[0]
     assert k2 == k1 + 1  # the separate fold is one more launch
-    assert k0 == k1      # a small set folds in its items
-    for a, b, c in zip(ref, sep, auto):
-        for x, y, z in zip(a, b, c):
-            assert np.array_equal(x, y), f"workload {workload}: in-item fold differs from the fold launch"
+    assert k0 == k2      # the default is the fold launch
+    for g, (a, b, c) in enumerate(zip(ref, sep, auto)):
+        for what, x, y, z in zip(("fitness", "components"), a, b, c):
+            rel = float(np.max(np.abs(x - y) / np.abs(y)))
+            assert np.array_equal(x, y), (f"workload {workload}, generation {g}: {what} folded in the items differ "
+                                          f"from the fold launch (max rel {rel:.3e}, {int(np.sum(x != y))} values)")
             assert np.array_equal(x, z)
