@@ -230,19 +230,22 @@ __device__ __forceinline__ void cutoff_fn(float r1, float r2, float pf, float d,
 // scratch that precedes the staged geometry, in 16-byte units (bits 9-23),
 // whether the force scratch lives in global memory instead (bit 24), log2 of
 // the G of the configuration's default-rule tile (bits 25-27), whose summation
-// order every tile of a force item reproduces, and whether the item is a force
-// item (bit 28; energy/virial items otherwise).
+// order every tile of a force item reproduces, whether the item is a force
+// item (bit 28; energy/virial items otherwise) and, for an NN2B force item, whether its
+// configuration's bond list is symmetric, so that each unordered pair is evaluated once (bit 29).
 __host__ __device__ __forceinline__ int item_G(const WorkItem& it) { return it.G & 0xff; }
 __host__ __device__ __forceinline__ bool item_staged(const WorkItem& it) { return (it.G >> 8) & 1; }
 __host__ __device__ __forceinline__ size_t item_fbytes(const WorkItem& it) { return (size_t)((it.G >> 9) & 0x7fff) * 16; }
 __host__ __device__ __forceinline__ bool item_global(const WorkItem& it) { return (it.G >> 24) & 1; }
 __host__ __device__ __forceinline__ int item_Grule(const WorkItem& it) { return 1 << ((it.G >> 25) & 7); }
 __host__ __device__ __forceinline__ bool item_force(const WorkItem& it) { return (it.G >> 28) & 1; }
-__host__ __device__ __forceinline__ int pack_G(int G, bool staged, size_t fbytes, bool global, int Grule, bool force) {
+__host__ __device__ __forceinline__ bool item_pairs_once(const WorkItem& it) { return (it.G >> 29) & 1; }
+__host__ __device__ __forceinline__ int pack_G(int G, bool staged, size_t fbytes, bool global, int Grule, bool force,
+                                               bool once = false) {
   int lg = 0;
   while ((1 << lg) < (Grule ? Grule : G)) ++lg;
   return G | (staged ? 1 << 8 : 0) | (int)(((fbytes + 15) / 16) << 9) | (global ? 1 << 24 : 0) | (lg << 25) |
-         (force ? 1 << 28 : 0);
+         (force ? 1 << 28 : 0) | (once ? 1 << 29 : 0);
 }
 
 // Fixed-order fold of per-lane partial sums held in shared memory as
@@ -1270,11 +1273,11 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
       __pipeline_commit();
     }
   } else {
-    for (int il = warp; il < Na; il += kWarps) {
-      int bbeg, bend;
-      bond_range(il, bbeg, bend);
-      // two pairs per weight load up to 16 neurons (registers allow it), one above
-      constexpr int NP = NMAX <= 16 ? 2 : 1;
+    // the pairs of one bond range through the MLP: each pair's tapered energy and radial
+    // derivative go to use(bond, geometry, p2, fd); two pairs per weight load up to 16 neurons
+    // (registers allow it), one above
+    constexpr int NP = NMAX <= 16 ? 2 : 1;
+    auto eval_range = [&](int bbeg, int bend, auto&& use) {
       for (int b = bbeg; b < bend; b += NP) {
         float4 q[NP];
         float d[NP], p2[NP], f2raw[NP];
@@ -1308,11 +1311,43 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
               pu *= fc;
               fd = f2raw[u] * fc + pu * fcp;
             }
-            consume(ks, q[u], pu, fd);
+            use(b + u, q[u], pu, fd);
           }
         }
       }
-      finish_atom(il, ks);
+    };
+    if constexpr (FORCE) {
+      // Force items evaluate the pairs into the item's scratch [bond][individual] in global
+      // memory, then gather F_i = sum_j fd u_ij over i's full list in list order.  When the
+      // configuration's bond list is symmetric (every bond's reverse is the same pair with the
+      // negated vector, hence the same FP32 length; item_pairs_once), each unordered pair is
+      // evaluated once, from its lower atom, and the gather reads the reverse bond's slot for
+      // j < i: the same terms in the same order as evaluating every directed pair, with half the
+      // network evaluations.  Otherwise every directed pair is evaluated into its own slot.
+      float* __restrict__ scr = J.gscratch + (size_t)it.gofs * 64;
+      const int bond0 = S.off[atom0];
+      const bool once = item_pairs_once(it);
+      for (int il = warp; il < Na; il += kWarps) {
+        const int i = atom0 + il;
+        eval_range(once ? S.half_off[i] : S.off[i], S.off[i + 1],
+                   [&](int b, const float4&, float, float fd) { scr[(size_t)(b - bond0) * 32 + lane] = fd; });
+      }
+      __syncthreads();  // every pair's fd is in the scratch (plain loads below: written by this launch)
+      for (int il = warp; il < Na; il += kWarps) {
+        const int i = atom0 + il;
+        for (int b = S.off[i]; b < S.off[i + 1]; ++b) {
+          const int cb = once && S.nbr[b] < i ? S.rev[b] : b;
+          consume(ks, __ldg(&S.g32[b]), 0.f, scr[(size_t)(cb - bond0) * 32 + lane]);
+        }
+        finish_atom(il, ks);
+      }
+    } else {
+      for (int il = warp; il < Na; il += kWarps) {
+        int bbeg, bend;
+        bond_range(il, bbeg, bend);
+        eval_range(bbeg, bend, [&](int, const float4& q, float pu, float fd) { consume(ks, q, pu, fd); });
+        finish_atom(il, ks);
+      }
     }
   }
   reduce_item<32>(it, P, S.Nc, acc, smem, res);  // pair items hold 32 individuals
@@ -1320,13 +1355,16 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
 
 // RI: three CTAs per SM (at most 85 registers); NN2B: two (128 registers, two pairs per weight
 // load) -- each measured faster than the unbounded register allocation, and than NN2B at three
-// CTAs per SM (with either one or two pairs per weight load).  One launch holds both kinds of items.
-template <int KIND, int NMAX>
+// CTAs per SM (with either one or two pairs per weight load).  NN2B's two kinds of items share a
+// launch; the rigid ion's go in two launches of single-kind instantiations (job_items).
+// ONLY: 0 both kinds of items (item_force), 1 force items only, 2 energy/virial items only (one
+// body, so its own register allocation).
+template <int KIND, int NMAX, int ONLY>
 __global__ void __launch_bounds__(kBlock, KIND == 1 ? 3 : 2) pair_batched(const JobView* __restrict__ jobs,
                                                                          const WorkItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem[];
   const WorkItem it = items[blockIdx.x];
-  if (item_force(it))
+  if (ONLY == 1 || (ONLY == 0 && item_force(it)))
     pair_item<KIND, NMAX, true>(jobs, it, smem);
   else
     pair_item<KIND, NMAX, false>(jobs, it, smem);
@@ -1382,6 +1420,8 @@ DevView make_view(const DevSet& d) {
   v.NN = d.NN;
   v.off = d.off;
   v.half_off = d.half_off;
+  v.nbr = d.nbr;
+  v.rev = d.rev;
   v.rev_sm = d.rev_sm;
   v.ptype = d.ptype;
   v.g32 = d.g32;
@@ -1549,6 +1589,22 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
       atom_sfu_half[i] = spp * half;
     }
   }
+  // NN2B force configurations whose bond list is symmetric (bond i -> j implies j -> i; the
+  // nearest-image rule gives that except at exact half-box ties): their force items evaluate each
+  // unordered pair once (pair_item)
+  std::vector<char> pair_sym;
+  if (kind == 2) {
+    pair_sym.assign(ts.Nc, 0);
+    for (int c = 0; c < ts.Nc_force; ++c) {
+      bool sym = true;
+      for (int i = ts.Na_sum[c]; sym && i < ts.Na_sum[c] + ts.Na[c]; ++i)
+        for (int b = e->h_off[i]; sym && b < e->h_off[i + 1]; ++b) {
+          const int j = e->h_nbr[b];
+          sym = j != i && std::binary_search(e->h_nbr.begin() + e->h_off[j], e->h_nbr.begin() + e->h_off[j + 1], i);
+        }
+      pair_sym[c] = sym;
+    }
+  }
   for (int c = 0; c < ts.Nc; ++c) {
     if (only && !(*only)[c]) continue;
     const bool force = c < ts.Nc_force;
@@ -1556,7 +1612,7 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
     const int mode = (modes && !modes->empty() && (*modes)[c] > 0) ? (*modes)[c] : kTileDefault;
     int zc = 0, G = 32, Grule = 32;
     size_t smem = kRedBytes;
-    bool staged = false, global = false;
+    bool staged = false, global = false, once = false;
     size_t fbytes = 0, item_floats = 0;
     if (kind == 0) {
       zc = zclass_of(e->h_zmax[c]);
@@ -1614,13 +1670,24 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
       }
     } else if (kind == 2) {
       smem += (size_t)32 * (nmax * nmax + 4 * nmax + 1) * sizeof(float);  // NNSmem<nmax>::floats
+      if (force) {
+        // the pairs' fd in a [bond][individual] global scratch, each unordered pair once when the
+        // bond list is symmetric
+        global = true;
+        once = pair_sym[c] != 0;
+        const long long Bc = (long long)e->h_off[ts.Na_sum[c] + Na] - e->h_off[ts.Na_sum[c]];
+        item_floats = ((size_t)Bc * 32 + 63) & ~(size_t)63;
+      }
     } else {
       smem += kPairStageBytes;  // RI: the warps' two-stage pair buffers
     }
-    const LaunchKey key{kind, zc, nmax, 0, lo ? 1 : 0};  // force and energy/virial items share launches
+    // force and energy/virial items share a launch, except the rigid ion's: its two bodies under
+    // one register allocation spilled more and ran 3 % slower than two single-kind kernels on two
+    // streams (300-configuration set: 5.92 vs 5.74 ms per generation)
+    const LaunchKey key{kind, zc, nmax, kind == 1 && force ? 1 : 0, lo ? 1 : 0};
     smem_need[key] = std::max(smem_need[key], smem);
     double cf = 0, cs = 0;
-    const bool half = kind != 0 && !force;
+    const bool half = kind != 0 && (!force || once);  // unordered pairs evaluated once
     for (int k = 0; k < Na; ++k) {
       const int i = ts.Na_sum[c] + k;
       cf += half ? atom_flops_half[i] : atom_flops[i];
@@ -1638,7 +1705,7 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
         *gscratch_floats += item_floats;
       }
       groups[key].push_back(
-          {WorkItem{c, p0, pack_G(G, staged, fbytes, global, Grule, force), job, gofs}, cf * cnt, (double)Na * cnt, cf * cnt, cs * cnt});
+          {WorkItem{c, p0, pack_G(G, staged, fbytes, global, Grule, force, once), job, gofs}, cf * cnt, (double)Na * cnt, cf * cnt, cs * cnt});
     }
   }
   return GPUGA_OK;
@@ -1671,20 +1738,21 @@ int launch_one(const LaunchSet* ls, const Launch& L, cudaStream_t st, bool confi
   do {                                                                                \
     if (L.nmax == 2) GPUGA_TERSOFF1(ZC, 2); else GPUGA_TERSOFF1(ZC, 1);               \
   } while (0)
-#define GPUGA_PAIR(KD, NM)                                                            \
+#define GPUGA_PAIR1(KD, NM, ON)                                                       \
   do {                                                                                \
     if (configure_only) {                                                             \
-      GPUGA_TRY(set_smem(pair_batched<KD, NM>));                                      \
+      GPUGA_TRY(set_smem(pair_batched<KD, NM, ON>));                                  \
       break;                                                                          \
     }                                                                                 \
-    pair_batched<KD, NM><<<grid, block, L.smem, st>>>(ls->d_jobs, items);             \
+    pair_batched<KD, NM, ON><<<grid, block, L.smem, st>>>(ls->d_jobs, items);         \
   } while (0)
+#define GPUGA_PAIR(KD, NM) GPUGA_PAIR1(KD, NM, 0)
   if (L.kind == 0) {
     if (L.zclass == 4) GPUGA_TERSOFF(4);
     else if (L.zclass == 8) GPUGA_TERSOFF(8);
     else GPUGA_TERSOFF(16);
-  } else if (L.kind == 1) {
-    GPUGA_PAIR(1, 8);
+  } else if (L.kind == 1) {  // the rigid ion's two kinds in launches of their own (job_items)
+    if (L.force == 1) GPUGA_PAIR1(1, 8, 1); else GPUGA_PAIR1(1, 8, 2);
   } else if (L.nmax == 8) {
     GPUGA_PAIR(2, 8);
   } else if (L.nmax == 12) {
@@ -1697,6 +1765,7 @@ int launch_one(const LaunchSet* ls, const Launch& L, cudaStream_t st, bool confi
 #undef GPUGA_TERSOFF
 #undef GPUGA_TERSOFF1
 #undef GPUGA_PAIR
+#undef GPUGA_PAIR1
   GPUGA_CUDA(cudaGetLastError());
   return GPUGA_OK;
 }

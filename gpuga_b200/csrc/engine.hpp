@@ -109,6 +109,8 @@ struct DevView {
   const int* NN;
   const int* off;
   const int* half_off;
+  const int* nbr;
+  const int* rev;
   const int* rev_sm;
   const uint8_t* ptype;
   const float4* g32;

@@ -91,7 +91,7 @@ struct Job {
 // per bond ~80 B (FP64 + FP32 geometry, indices, RI terms), per three-body
 // term 4 B, with the neighbor count estimated from the cell density.
 size_t estimate_bytes(const PotentialSpec& spec, const TrainingSet& ts, int P) {
-  double bonds = 0, trip = 0;
+  double bonds = 0, trip = 0, force_bonds = 0;
   const double rc = spec.cutoff;
   for (int c = 0; c < ts.Nc; ++c) {
     const float* h = ts.h.data() + 18 * (size_t)c;
@@ -101,11 +101,13 @@ size_t estimate_bytes(const PotentialSpec& spec, const TrainingSet& ts, int P) {
     double z = vol > 0 ? na / vol * 4.18879 * rc * rc * rc : na - 1;
     z = std::min(z, na - 1.0);
     bonds += na * z;
+    if (c < ts.Nc_force) force_bonds += na * z;
     trip += na * z * z;
   }
   const bool tersoff = spec.type == 1 || spec.type == 2;
   double bytes = 64.0 * ts.N + 88.0 * bonds + (tersoff ? 4.0 * trip : 0.0);
   bytes += (double)P * ts.Nc * kResK * 8.0 + (double)P * (spec.num_vars + 40) * 8.0;
+  if (spec.type == 3) bytes += 4.0 * P * force_bonds;  // NN2B force items' per-pair scratch
   return (size_t)(1.25 * bytes) + (8u << 20);
 }
 
