@@ -1322,7 +1322,7 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
       // configuration's bond list is symmetric (every bond's reverse is the same pair with the
       // negated vector, hence the same FP32 length; item_pairs_once), each unordered pair is
       // evaluated once, from its lower atom, and the gather reads the reverse bond's slot for
-      // j < i: the same terms in the same order as evaluating every directed pair, with half the
+      // j < i (DevView::pslot): the same terms in the same order as evaluating every directed pair, with half the
       // network evaluations.  Otherwise every directed pair is evaluated into its own slot.
       float* __restrict__ scr = J.gscratch + (size_t)it.gofs * 64;
       const int bond0 = S.off[atom0];
@@ -1335,9 +1335,11 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
       __syncthreads();  // every pair's fd is in the scratch (plain loads below: written by this launch)
       for (int il = warp; il < Na; il += kWarps) {
         const int i = atom0 + il;
-        for (int b = S.off[i]; b < S.off[i + 1]; ++b) {
-          const int cb = once && S.nbr[b] < i ? S.rev[b] : b;
-          consume(ks, __ldg(&S.g32[b]), 0.f, scr[(size_t)(cb - bond0) * 32 + lane]);
+        const int be = S.off[i + 1];
+#pragma unroll 4
+        for (int b = S.off[i]; b < be; ++b) {
+          const int cb = once ? __ldg(&S.pslot[b]) : b - bond0;
+          consume(ks, __ldg(&S.g32[b]), 0.f, scr[(size_t)cb * 32 + lane]);
         }
         finish_atom(il, ks);
       }
@@ -1420,8 +1422,7 @@ DevView make_view(const DevSet& d) {
   v.NN = d.NN;
   v.off = d.off;
   v.half_off = d.half_off;
-  v.nbr = d.nbr;
-  v.rev = d.rev;
+  v.pslot = d.pslot;
   v.rev_sm = d.rev_sm;
   v.ptype = d.ptype;
   v.g32 = d.g32;

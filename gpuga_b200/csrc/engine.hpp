@@ -53,6 +53,7 @@ struct DevSet {
   int* half_off = nullptr;
   int* nbr = nullptr;
   int* rev = nullptr;
+  int* pslot = nullptr;  // NN2B: each bond's pair-derivative slot in a force item's scratch
   int* rev_sm = nullptr;
   uint8_t* ptype = nullptr;
   float4* g32 = nullptr;
@@ -109,8 +110,7 @@ struct DevView {
   const int* NN;
   const int* off;
   const int* half_off;
-  const int* nbr;
-  const int* rev;
+  const int* pslot;
   const int* rev_sm;
   const uint8_t* ptype;
   const float4* g32;

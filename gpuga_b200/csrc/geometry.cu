@@ -240,6 +240,18 @@ __global__ void bond_geometry(int N, const int* __restrict__ atom_cfg, const flo
   half_off[i] = hstart;
 }
 
+// NN2B: the slot each bond's pair derivative is read from in a force item's scratch, local to
+// the configuration's first bond: the bond itself when its neighbor has a larger index, else its
+// reverse (the unordered pair is evaluated from its lower atom).
+__global__ void pair_slots(int N, const int* __restrict__ atom_cfg, const int* __restrict__ Na_sum,
+                           const int* __restrict__ off, const int* __restrict__ nbr, const int* __restrict__ rev,
+                           int* __restrict__ pslot) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int bond0 = off[Na_sum[atom_cfg[i]]];
+  for (int b = off[i]; b < off[i + 1]; ++b) pslot[b] = (nbr[b] > i ? b : rev[b]) - bond0;
+}
+
 // Position of each bond's reverse in the batched force kernel's slot-major
 // scratch of its configuration: slot * Na + atom, both local to the configuration.
 __global__ void reverse_slots(int N, const int* __restrict__ atom_cfg, const int* __restrict__ Na,
@@ -677,6 +689,11 @@ int build_geometry(Engine* e) {
   GPUGA_TRY(e->alloc(&d.rev_sm, std::max(B, 1)));
   reverse_slots<<<(N + 127) / 128, 128, 0, st>>>(N, d_atom_cfg, d.Na, d.Na_sum, d.off, d.nbr, d.rev, d.rev_sm);
   GPUGA_CUDA(cudaGetLastError());
+  if (d.potential_type == 3) {
+    GPUGA_TRY(e->alloc(&d.pslot, std::max(B, 1)));
+    pair_slots<<<(N + 127) / 128, 128, 0, st>>>(N, d_atom_cfg, d.Na_sum, d.off, d.nbr, d.rev, d.pslot);
+    GPUGA_CUDA(cudaGetLastError());
+  }
   if (ri) {
     d.ri_active = ri_active_types(e->spec);
     std::vector<int> half(N), start(N + 1, 0);
