@@ -1273,17 +1273,20 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
       __pipeline_commit();
     }
   } else {
-    // the pairs of one bond range through the MLP: each pair's tapered energy and radial
-    // derivative go to use(bond, geometry, p2, fd); two pairs per weight load up to 16 neurons
-    // (registers allow it), one above
+    // pairs through the MLP: each pair's tapered energy and radial derivative go to
+    // use(bond, geometry, p2, fd); two pairs per weight load up to 16 neurons (registers allow
+    // it), one above
     constexpr int NP = NMAX <= 16 ? 2 : 1;
-    auto eval_range = [&](int bbeg, int bend, auto&& use) {
-      for (int b = bbeg; b < bend; b += NP) {
+    // bond_of(k) for k in [kbeg, kend) in steps of `step`: the bonds to evaluate
+    auto eval_list = [&](int kbeg, int kend, int step, auto&& bond_of, auto&& use) {
+      for (int b = kbeg; b < kend; b += step) {
         float4 q[NP];
         float d[NP], p2[NP], f2raw[NP];
+        int bd[NP];
 #pragma unroll
         for (int u = 0; u < NP; ++u) {
-          q[u] = __ldg(&S.g32[min(b + u, bend - 1)]);
+          bd[u] = bond_of(min(b + u, kend - 1));
+          q[u] = __ldg(&S.g32[bd[u]]);
           d[u] = q[u].w;
         }
         // force items: p2 enters only through the taper derivative (warp-uniform test: the
@@ -1300,7 +1303,7 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
           nn_pairs<NMAX, NP, 0>(wsm, lane, nn, d, need_p2, p2, f2raw);
 #pragma unroll
         for (int u = 0; u < NP; ++u) {
-          if (b + u < bend) {
+          if (b + u < kend) {
             float fc, fcp, fd;
             cutoff_fn(tp.r1, tp.r2, tp.pf, d[u], fc, fcp);
             float pu = p2[u];
@@ -1311,7 +1314,7 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
               pu *= fc;
               fd = f2raw[u] * fc + pu * fcp;
             }
-            use(b + u, q[u], pu, fd);
+            use(bd[u], q[u], pu, fd);
           }
         }
       }
@@ -1324,14 +1327,17 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
       // evaluated once, from its lower atom, and the gather reads the reverse bond's slot for
       // j < i (DevView::pslot): the same terms in the same order as evaluating every directed pair, with half the
       // network evaluations.  Otherwise every directed pair is evaluated into its own slot.
+      // Pass 1 takes the configuration's list of bonds to evaluate (DevView::hb) in consecutive
+      // groups of NP per warp: balanced across warps, and one partial group per configuration
+      // instead of one per atom.
       float* __restrict__ scr = J.gscratch + (size_t)it.gofs * 64;
       const int bond0 = S.off[atom0];
       const bool once = item_pairs_once(it);
-      for (int il = warp; il < Na; il += kWarps) {
-        const int i = atom0 + il;
-        eval_range(once ? S.half_off[i] : S.off[i], S.off[i + 1],
-                   [&](int b, const float4&, float, float fd) { scr[(size_t)(b - bond0) * 32 + lane] = fd; });
-      }
+      const int* __restrict__ hb = S.hb + S.hb_off[c];
+      const int nh = S.hb_off[c + 1] - S.hb_off[c];
+      for (int k0 = warp * NP; k0 < nh; k0 += kWarps * NP)
+        eval_list(k0, min(k0 + NP, nh), NP, [&](int k) { return __ldg(&hb[k]); },
+                  [&](int b, const float4&, float, float fd) { scr[(size_t)(b - bond0) * 32 + lane] = fd; });
       __syncthreads();  // every pair's fd is in the scratch (plain loads below: written by this launch)
       for (int il = warp; il < Na; il += kWarps) {
         const int i = atom0 + il;
@@ -1347,7 +1353,8 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
       for (int il = warp; il < Na; il += kWarps) {
         int bbeg, bend;
         bond_range(il, bbeg, bend);
-        eval_range(bbeg, bend, [&](int, const float4& q, float pu, float fd) { consume(ks, q, pu, fd); });
+        eval_list(bbeg, bend, NP, [](int k) { return k; },
+                  [&](int, const float4& q, float pu, float fd) { consume(ks, q, pu, fd); });
         finish_atom(il, ks);
       }
     }
@@ -1423,6 +1430,8 @@ DevView make_view(const DevSet& d) {
   v.off = d.off;
   v.half_off = d.half_off;
   v.pslot = d.pslot;
+  v.hb = d.hb;
+  v.hb_off = d.hb_off;
   v.rev_sm = d.rev_sm;
   v.ptype = d.ptype;
   v.g32 = d.g32;
@@ -1590,22 +1599,9 @@ int job_items(const Engine* e, int P, int job, std::map<LaunchKey, std::vector<I
       atom_sfu_half[i] = spp * half;
     }
   }
-  // NN2B force configurations whose bond list is symmetric (bond i -> j implies j -> i; the
-  // nearest-image rule gives that except at exact half-box ties): their force items evaluate each
-  // unordered pair once (pair_item)
-  std::vector<char> pair_sym;
-  if (kind == 2) {
-    pair_sym.assign(ts.Nc, 0);
-    for (int c = 0; c < ts.Nc_force; ++c) {
-      bool sym = true;
-      for (int i = ts.Na_sum[c]; sym && i < ts.Na_sum[c] + ts.Na[c]; ++i)
-        for (int b = e->h_off[i]; sym && b < e->h_off[i + 1]; ++b) {
-          const int j = e->h_nbr[b];
-          sym = j != i && std::binary_search(e->h_nbr.begin() + e->h_off[j], e->h_nbr.begin() + e->h_off[j + 1], i);
-        }
-      pair_sym[c] = sym;
-    }
-  }
+  // NN2B force configurations whose bond list is symmetric (engine set-up, geometry.cu): their
+  // force items evaluate each unordered pair once (pair_item)
+  const std::vector<char>& pair_sym = e->h_pair_sym;
   for (int c = 0; c < ts.Nc; ++c) {
     if (only && !(*only)[c]) continue;
     const bool force = c < ts.Nc_force;

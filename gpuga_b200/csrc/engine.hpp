@@ -54,6 +54,8 @@ struct DevSet {
   int* nbr = nullptr;
   int* rev = nullptr;
   int* pslot = nullptr;  // NN2B: each bond's pair-derivative slot in a force item's scratch
+  int* hb = nullptr;     // NN2B: per force configuration the bonds its force items evaluate
+  int* hb_off = nullptr; //   (each unordered pair once where the list is symmetric), [Nc + 1]
   int* rev_sm = nullptr;
   uint8_t* ptype = nullptr;
   float4* g32 = nullptr;
@@ -111,6 +113,8 @@ struct DevView {
   const int* off;
   const int* half_off;
   const int* pslot;
+  const int* hb;
+  const int* hb_off;
   const int* rev_sm;
   const uint8_t* ptype;
   const float4* g32;
@@ -246,6 +250,7 @@ struct Engine {
   float* d_pmin = nullptr;
   float* d_pmax = nullptr;
   std::vector<int> h_NN, h_off, h_nbr, h_zmax;  // host copies of the neighbor list
+  std::vector<char> h_pair_sym;                 // NN2B: per configuration, bond list symmetric
   std::map<int, std::unique_ptr<Plan>> plans;    // keyed by population size
   size_t device_bytes = 0;
   std::vector<void*> allocations;
