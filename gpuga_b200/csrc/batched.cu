@@ -1192,11 +1192,6 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
 #pragma unroll
     for (int k = 0; k < NK; ++k) ks[k] = KSum{};
   };
-  auto bond_range = [&](int il, int& bb, int& be) {
-    const int i = atom0 + il;
-    bb = FORCE ? S.off[i] : S.half_off[i];
-    be = S.off[i + 1];
-  };
   KSum ks[NK];
   if constexpr (KIND == 1) {
     // The warp's pairs (atoms warp, warp + 8, ... and each atom's bonds) stream through a
@@ -1350,13 +1345,21 @@ __device__ __forceinline__ void pair_item(const JobView* __restrict__ jobs, cons
         finish_atom(il, ks);
       }
     } else {
-      for (int il = warp; il < Na; il += kWarps) {
-        int bbeg, bend;
-        bond_range(il, bbeg, bend);
-        eval_list(bbeg, bend, NP, [](int k) { return k; },
+      // energy/virial items need the configuration's totals only: consecutive groups of the
+      // unordered-pair list per warp, the compensated energy and FMA virial sums flushed to FP64
+      // every 16 groups (FP32 chains as short as an atom's half list)
+      const int* __restrict__ hb = S.hb + S.hb_off[c];
+      const int nh = S.hb_off[c + 1] - S.hb_off[c];
+      int groups = 0;
+      for (int k0 = warp * NP; k0 < nh; k0 += kWarps * NP) {
+        eval_list(k0, min(k0 + NP, nh), NP, [&](int k) { return __ldg(&hb[k]); },
                   [&](int, const float4& q, float pu, float fd) { consume(ks, q, pu, fd); });
-        finish_atom(il, ks);
+        if (++groups == 16) {
+          groups = 0;
+          finish_atom(0, ks);
+        }
       }
+      finish_atom(0, ks);
     }
   }
   reduce_item<32>(it, P, S.Nc, acc, smem, res);  // pair items hold 32 individuals

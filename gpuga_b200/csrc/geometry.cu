@@ -749,16 +749,22 @@ int build_geometry(Engine* e) {
     for (int k = 0; k < ts.Na[c]; ++k) e->h_zmax[c] = std::max(e->h_zmax[c], e->h_NN[ts.Na_sum[c] + k]);
   if (tersoff) GPUGA_TRY(build_slot_major(e, st));
   if (d.potential_type == 3) {
-    // NN2B force configurations: the bonds whose pair derivative a force item evaluates, as one
-    // list per configuration (hb, hb_off).  When the configuration's bond list is symmetric (every
-    // bond's reverse present: the nearest-image rule gives that except at exact half-box ties)
-    // those are the bonds to a higher-index neighbor -- each unordered pair once -- else all bonds.
+    // NN2B: the bonds each configuration's work items evaluate, as one list per configuration
+    // (hb, hb_off).  Energy/virial configurations: the bonds to a higher-index neighbor (the
+    // unordered pairs).  Force configurations: the same when the bond list is symmetric (every
+    // bond's reverse present: the nearest-image rule gives that except at exact half-box ties),
+    // else all bonds.
     e->h_pair_sym.assign(Nc, 0);
     std::vector<int> hb, hb_off(Nc + 1, 0);
     for (int c = 0; c < Nc; ++c) {
       hb_off[c] = (int)hb.size();
-      if (c >= ts.Nc_force) continue;
       const int a0 = ts.Na_sum[c], a1 = a0 + ts.Na[c];
+      if (c >= ts.Nc_force) {  // energy/virial items: the unordered pairs (the half lists)
+        for (int i = a0; i < a1; ++i)
+          for (int b = e->h_off[i]; b < e->h_off[i + 1]; ++b)
+            if (e->h_nbr[b] > i) hb.push_back(b);
+        continue;
+      }
       bool sym = true;
       for (int i = a0; sym && i < a1; ++i)
         for (int b = e->h_off[i]; sym && b < e->h_off[i + 1]; ++b) {
