@@ -20,7 +20,9 @@ GENS = 6
 @pytest.fixture(scope="module")
 def job_dirs(built_oracle, tmp_path_factory):
     dirs = []
-    for cfg, Nc, P in [(1, 8, 40), (2, 12, 60), (3, 4, 20), (1, 6, 40)]:  # parent_number = P/2, a multiple of 10
+    # parent_number = P/2, a multiple of 10; the NN2B job (4) brings its per-pair scratch and pair
+    # lists into the shared launch sets
+    for cfg, Nc, P in [(1, 8, 40), (2, 12, 60), (3, 4, 20), (1, 6, 40), (4, 4, 20)]:
         d, data = synthetic_dir(built_oracle, cfg, Nc, str(tmp_path_factory.mktemp(f"job{cfg}_{Nc}")))
         with open(f"{d}/ga.in", "w") as f:
             f.write(f"maximum_generation 50\npopulation_size {P}\nparent_number {P // 2}\nmutation_rate 0.2\n")
@@ -50,7 +52,7 @@ def _pop_size(d):
 def test_jobs_are_the_same_alone_and_in_the_mix(job_dirs):
     refs = [alone(d, 1000 + k) for k, d in enumerate(job_dirs)]
     with Server(device=0, hbm_budget_bytes=120e9, max_jobs=32) as srv:
-        srv.hold(True)  # load every job first, so that all four share every window
+        srv.hold(True)  # load every job first, so that all of them share every window
         ids = [srv.submit(d, seed=1000 + k, generations=GENS) for k, d in enumerate(job_dirs)]
         deadline = time.time() + 120
         while any(srv.poll(j)[3] == Server.QUEUED for j in ids) and time.time() < deadline:
@@ -59,7 +61,7 @@ def test_jobs_are_the_same_alone_and_in_the_mix(job_dirs):
         assert srv.drain(300) == _lib.OK
         st = srv.stats()
         assert st["jobs_finished"] == len(job_dirs)
-        assert st["peak_resident_jobs"] == len(job_dirs)  # all four shared the launches
+        assert st["peak_resident_jobs"] == len(job_dirs)  # all of them shared the launches
         assert st["batches"] == GENS
         assert st["p99_gen_ms"] >= st["p50_gen_ms"] > 0
         assert st["p99_wall_gen_ms"] >= st["p50_wall_gen_ms"] > 0
