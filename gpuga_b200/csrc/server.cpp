@@ -8,8 +8,9 @@
 //   (training set upload, neighbor lists, geometry), the population plan, the
 //   host GA (seeded RNG stream) and the device GA buffers, uploads the initial
 //   population and hands the job to the scheduler as "ready".  It also frees
-//   the device memory of finished jobs and of retired launch sets, so that no
-//   cudaFree (which waits for the device) runs on the scheduler thread.
+//   the device memory of finished jobs and (when nothing is resident, or 64 have
+//   accumulated) of retired launch sets, so that no cudaFree (which waits for the
+//   device) runs on the scheduler thread or between the windows of a busy period.
 //
 //   Scheduler thread.  Owns one stream and runs all resident jobs together in
 //   windows of up to kWindow generations.  Each generation is one CUDA graph:
@@ -138,6 +139,7 @@ double percentile(std::vector<double> t, double q) {
 // Generations per scheduling window (admission, retirement and cancellation
 // happen at window boundaries).
 constexpr int kWindow = 8;
+constexpr size_t kRetiredBacklog = 64;  // retired launch sets kept before the loader frees them
 
 struct gpuga_server {
   int device = 0;
@@ -224,11 +226,17 @@ void gpuga_server::load() {
   cudaSetDevice(device);
   std::unique_lock<std::mutex> lock(mu);
   while (true) {
-    if (!graveyard.empty() || !retired.empty()) {
+    // Retired launch sets (a few MB each) are freed only when the scheduler has nothing resident
+    // or a backlog has built up: every cudaFree waits for the device to drain, and one per
+    // admission would stall the windows in flight.  Finished jobs are freed at once (their
+    // memory goes back to the admission budget).
+    const bool idle = running.empty() && ready.empty() && loading == 0;
+    const bool free_retired = !retired.empty() && (idle || stop || retired.size() >= kRetiredBacklog);
+    if (!graveyard.empty() || free_retired) {
       std::vector<Job*> dead;
       dead.swap(graveyard);
       std::vector<std::unique_ptr<Batch>> old;
-      old.swap(retired);
+      if (free_retired) old.swap(retired);
       lock.unlock();
       old.clear();
       for (Job* j : dead) {
