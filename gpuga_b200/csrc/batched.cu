@@ -371,37 +371,27 @@ __device__ __forceinline__ Geo stage_geometry(const DevView& S, int c, int atom0
 //
 // FULL: every one of the ZC bond slots is present (Z == ZC, e.g. all atoms of a diamond
 // lattice), so that the per-slot guards fold away at compile time.
-template <int ZC, int NT, bool FORCE, bool FULL, bool LO, int PM, class GEO>
-__device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C, int il, int Na, float* fsm, int G,
-                                               int g, float (&v)[6]) {
-  const int Z = FULL ? ZC : geo.nn[il];
-  const int b0 = geo.base(il), bs = geo.step();  // bond j at b0 + j * bs
-  float ux[ZC], uy[ZC], uz[ZC], dd[ZC];
-  double d64[PM == kPair64 ? ZC : 1];  // FP64 lengths, loaded with the rest of the geometry
-  int st[ZC];
-#pragma unroll
-  for (int j = 0; j < ZC; ++j) {
-    st[j] = 0;
-    if (j < Z) {
-      const float4 q = geo.g[b0 + j * bs];
-      ux[j] = q.x;
-      uy[j] = q.y;
-      uz[j] = q.z;
-      dd[j] = q.w;
-      if constexpr (PM == kPair64) d64[j] = geo.d64[b0 + j * bs];
-      if (NT == 2) st[j] = geo.pt[b0 + j * bs];
-    } else {
-      ux[j] = uy[j] = uz[j] = 0.f;
-      dd[j] = 1.0f;
-      if constexpr (PM == kPair64) d64[j] = 1.0;
-    }
-  }
+//
+// INNER: every bond of the atom lies inside r1 (fc = 1, fc' = 0; most atoms of a set near
+// equilibrium), so that the cutoff branches and the fc' terms drop out.  The expressions that
+// involve fc or fc' are written with explicit roundings, so that for such an atom both forms give
+// the same bits: the force-item tiles, which group atoms into warps differently, stay identical.
+template <int ZC, int NT, bool FORCE, bool FULL, bool LO, int PM, bool INNER, class GEO>
+__device__ __forceinline__ double tersoff_bonds(const GEO& geo, const TersoffC& C, int il, int Na, float* fsm, int G,
+                                                int g, float (&v)[6], int Z, int b0, int bs, const float (&ux)[ZC],
+                                                const float (&uy)[ZC], const float (&uz)[ZC], const float (&dd)[ZC],
+                                                const double (&d64)[PM == kPair64 ? ZC : 1], const int (&st)[ZC]) {
   // pass A: cutoff of every bond
   float fc[ZC], fcp[ZC];
 #pragma unroll
   for (int j = 0; j < ZC; ++j) {
-    fc[j] = fcp[j] = 0.f;
-    if (j < Z) cutoff_fn(C.r1, C.r2, C.pf, dd[j], fc[j], fcp[j]);
+    if constexpr (INNER) {
+      fc[j] = 1.0f;
+      fcp[j] = 0.0f;
+    } else {
+      fc[j] = fcp[j] = 0.f;
+      if (j < Z) cutoff_fn(C.r1, C.r2, C.pf, dd[j], fc[j], fcp[j]);
+    }
   }
   // pass B: bond order, site energy and the per-bond force scalars
   // cos(theta_jik) = u_j . u_k from the FP32 unit vectors (as accurate as a stored FP32 cosine);
@@ -435,23 +425,26 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
           zeta = fmaf(fc[k] * C.beta, x * x, zeta);
         }
       }
-      float b = 1.f, bp = 0.f;
-      if (!(zeta < 1.0e-16f)) {  // minimal_tersoff.cu:178-185
-        // Force items: FP32 log2f / exp2f (the same fitness error on the 500-configuration Si
-        // set, random and near-optimum individuals, and 11 % less time per generation);
-        // energy/virial items: powf_dd (double-float log2 and exponent)
-        float zn, opz;
-        if constexpr (PM == kPair32) {
-          zn = exp2f(C.en * log2f(zeta));
-          opz = 1.0f + zn;
-          const float lg = log2f(opz);
-          b = exp2f(fmaf(C.mhon, lg, C.mhonl * lg));
-        } else {
-          zn = powf_dd(zeta, C.en);
-          opz = 1.0f + zn;
-          b = powf_dd(opz, C.mhon, C.mhonl);
-        }
-        bp = __fdividef(-0.5f * b * zn, opz * zeta);
+      // b = 1, b' = 0 below zeta = 1e-16 (minimal_tersoff.cu:178-185), selected after the
+      // evaluation rather than branched around it (the threshold is almost never met).
+      // Force items: FP32 log2f / exp2f (the same fitness error on the 500-configuration Si
+      // set, random and near-optimum individuals, and 11 % less time per generation);
+      // energy/virial items: powf_dd (double-float log2 and exponent)
+      float zn, opz, b;
+      if constexpr (PM == kPair32) {
+        zn = exp2f(C.en * log2f(zeta));
+        opz = 1.0f + zn;
+        const float lg = log2f(opz);
+        b = exp2f(fmaf(C.mhon, lg, C.mhonl * lg));
+      } else {
+        zn = powf_dd(zeta, C.en);
+        opz = 1.0f + zn;
+        b = powf_dd(opz, C.mhon, C.mhonl);
+      }
+      float bp = __fdividef(-0.5f * b * zn, opz * zeta);
+      if (zeta < 1.0e-16f) {
+        b = 1.f;
+        bp = 0.f;
       }
       // pair terms fr = cr e^{-lr t}, fa = ca e^{-la t}, t = d - r0.  With S = 2 (!LO) lr = 2 la
       // and cr = ca / 2, so fr = fa e^{-la t} / 2 from the one exponential.
@@ -476,7 +469,7 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
           e = fma(-bd, fa, fr);
           dA = -la * (e + fr);
         }
-        if (fc[j] == 1.0f && fcp[j] == 0.0f) {  // inside r1: no conversions of fc, fc'
+        if (INNER || (fc[j] == 1.0f && fcp[j] == 0.0f)) {  // inside r1: no conversions of fc, fc'
           pe = fma(0.5, e, pe);
           Ap[j] = (float)dA;
         } else {
@@ -514,7 +507,9 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
         }
         const float e = fr - b * fa;
         pe32 = fmaf(0.5f * fc[j], e, pe32);
-        Ap[j] = fcp[j] * e + fc[j] * (frp - b * fap);
+        const float dA = __fmaf_rn(-b, fap, frp);  // fr' - b fa'
+        if constexpr (INNER) Ap[j] = dA;
+        else Ap[j] = __fmaf_rn(fcp[j], e, __fmul_rn(fc[j], dA));
         fa32 = fa;
       }
       Sb[j] = bp * fa32;
@@ -532,9 +527,10 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
         if (k < Z && k != j) {
           const float cjk = cosine(j, k);
           const float bx = C.beta * (cjk - C.h);
-          const float g = bx * (cjk - C.h);
-          const float q = bx * fmaf(Sj, fc[k], Tb[k]);
-          sumG = fmaf(Tb[k], g, sumG);
+          // S_j fc_k + T_k: with fc_k = 1 an explicit add (a folded fmaf(S_j, 1, T_k) could be
+          // contracted with the products S_j, T_k, unlike the general form)
+          const float q = bx * (INNER ? __fadd_rn(Sj, Tb[k]) : __fmaf_rn(Sj, fc[k], Tb[k]));
+          if constexpr (!INNER) sumG = fmaf(Tb[k], bx * (cjk - C.h), sumG);
           accC = fmaf(q, cjk, accC);
           Vx = fmaf(q, ux[k], Vx);
           Vy = fmaf(q, uy[k], Vy);
@@ -542,7 +538,7 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
         }
       }
       const float m = __fdividef(-2.0f * fc[j], dd[j]);
-      const float cu = 0.5f * (Ap[j] - fcp[j] * sumG - m * accC);
+      const float cu = 0.5f * __fmaf_rn(-m, accC, INNER ? Ap[j] : __fmaf_rn(-fcp[j], sumG, Ap[j]));
       const float cv = 0.5f * m;
       const float fx = fmaf(cu, ux[j], cv * Vx);
       const float fy = fmaf(cu, uy[j], cv * Vy);
@@ -566,6 +562,44 @@ __device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C
     }
   }
   return pe + (double)pe32;
+}
+
+template <int ZC, int NT, bool FORCE, bool FULL, bool LO, int PM, class GEO>
+__device__ __forceinline__ double tersoff_atom(const GEO& geo, const TersoffC& C, int il, int Na, float* fsm, int G,
+                                               int g, float (&v)[6]) {
+  const int Z = FULL ? ZC : geo.nn[il];
+  const int b0 = geo.base(il), bs = geo.step();  // bond j at b0 + j * bs
+  float ux[ZC], uy[ZC], uz[ZC], dd[ZC];
+  double d64[PM == kPair64 ? ZC : 1];  // FP64 lengths, loaded with the rest of the geometry
+  int st[ZC];
+#pragma unroll
+  for (int j = 0; j < ZC; ++j) {
+    st[j] = 0;
+    if (j < Z) {
+      const float4 q = geo.g[b0 + j * bs];
+      ux[j] = q.x;
+      uy[j] = q.y;
+      uz[j] = q.z;
+      dd[j] = q.w;
+      if constexpr (PM == kPair64) d64[j] = geo.d64[b0 + j * bs];
+      if (NT == 2) st[j] = geo.pt[b0 + j * bs];
+    } else {
+      ux[j] = uy[j] = uz[j] = 0.f;
+      dd[j] = 1.0f;
+      if constexpr (PM == kPair64) d64[j] = 1.0;
+    }
+  }
+  if constexpr (FULL) {
+    bool inside = true;
+#pragma unroll
+    for (int j = 0; j < ZC; ++j) inside = inside && dd[j] < C.r1;
+    // the lanes that reach this point take one form together
+    if (__all_sync(__activemask(), inside))
+      return tersoff_bonds<ZC, NT, FORCE, FULL, LO, PM, true>(geo, C, il, Na, fsm, G, g, v, Z, b0, bs, ux, uy, uz, dd,
+                                                               d64, st);
+  }
+  return tersoff_bonds<ZC, NT, FORCE, FULL, LO, PM, false>(geo, C, il, Na, fsm, G, g, v, Z, b0, bs, ux, uy, uz, dd,
+                                                            d64, st);
 }
 
 // Energy/virial items (FORCE = false) keep their FP64 per-lane sums in shared

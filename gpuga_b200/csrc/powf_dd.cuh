@@ -62,11 +62,13 @@ GPUGA_HD float pdd_rcp(float t) {
 }
 
 GPUGA_HD float powf_dd(float x, float y, float y_lo = 0.0f) {
-  if (x != x) return x;  // NaN
+#ifndef __CUDA_ARCH__
+  if (x != x) return x;  // NaN (on the device: selected at the end, without a branch)
+#endif
   // x = 2^e m with m in [sqrt(1/2), sqrt(2))
   const int32_t ix = pdd_as_int(x);
   const int32_t e = (ix - 0x3f3504f3) >> 23;
-  const float m = pdd_as_float(ix - (e << 23));
+  const float m = pdd_as_float((int32_t)((uint32_t)ix - ((uint32_t)e << 23)));
   const float f = m - 1.0f;  // exact
   // s = f / (2 + f) as s_h + s_l; t_lo recovers the bit 2 + f may lose
   const float t = 2.0f + f;
@@ -109,7 +111,12 @@ GPUGA_HD float powf_dd(float x, float y, float y_lo = 0.0f) {
   u = fmaf(r, u, 6.931471805599453e-01f);
   const float p2 = fmaf(r, u, 1.0f);
   const float v = pdd_as_float(pdd_as_int(p2) + (int32_t)k * (1 << 23));
-  return fabsf(t_h) <= 125.0f ? v : (t_h > 0.0f ? INFINITY : 0.0f);
+  const float out = fabsf(t_h) <= 125.0f ? v : (t_h > 0.0f ? INFINITY : 0.0f);
+#ifdef __CUDA_ARCH__
+  return x != x ? x : out;
+#else
+  return out;
+#endif
 }
 
 }  // namespace gpuga
