@@ -539,11 +539,11 @@ __device__ __forceinline__ double tersoff_bonds(const GEO& geo, const TersoffC& 
       }
       const float m = __fdividef(-2.0f * fc[j], dd[j]);
       const float cu = 0.5f * __fmaf_rn(-m, accC, INNER ? Ap[j] : __fmaf_rn(-fcp[j], sumG, Ap[j]));
-      const float cv = 0.5f * m;
-      const float fx = fmaf(cu, ux[j], cv * Vx);
-      const float fy = fmaf(cu, uy[j], cv * Vy);
-      const float fz = fmaf(cu, uz[j], cv * Vz);
       if (FORCE) {
+        const float cv = 0.5f * m;
+        const float fx = fmaf(cu, ux[j], cv * Vx);
+        const float fy = fmaf(cu, uy[j], cv * Vy);
+        const float fz = fmaf(cu, uz[j], cv * Vz);
         // slot-major scratch [slot][atom][xyz][G]: the lanes of a warp (consecutive atoms,
         // same slot) write consecutive words
         const int bl = j * Na + il;
@@ -551,13 +551,18 @@ __device__ __forceinline__ double tersoff_bonds(const GEO& geo, const TersoffC& 
         fsm[(bl * 3 + 1) * G + g] = fy;
         fsm[(bl * 3 + 2) * G + g] = fz;
       } else {
-        const float rx = dd[j] * ux[j], ry = dd[j] * uy[j], rz = dd[j] * uz[j];
-        v[0] = fmaf(-rx, fx, v[0]);
-        v[1] = fmaf(-ry, fy, v[1]);
-        v[2] = fmaf(-rz, fz, v[2]);
-        v[3] = fmaf(-rx, fy, v[3]);
-        v[4] = fmaf(-ry, fz, v[4]);
-        v[5] = fmaf(-rz, fx, v[5]);
+        // -r_ij (x) f_ij = u_j (x) t_j with t_j = a u_j + fc_j V_j, a = -d_j cu_j (r_j = d_j u_j,
+        // f_ij = cu u_j + (m_j / 2) V_j and -d_j m_j / 2 = fc_j), components xx yy zz xy yz zx
+        const float a = -dd[j] * cu;
+        const float tx = INNER ? __fmaf_rn(a, ux[j], Vx) : __fmaf_rn(a, ux[j], __fmul_rn(fc[j], Vx));
+        const float ty = INNER ? __fmaf_rn(a, uy[j], Vy) : __fmaf_rn(a, uy[j], __fmul_rn(fc[j], Vy));
+        const float tz = INNER ? __fmaf_rn(a, uz[j], Vz) : __fmaf_rn(a, uz[j], __fmul_rn(fc[j], Vz));
+        v[0] = fmaf(ux[j], tx, v[0]);
+        v[1] = fmaf(uy[j], ty, v[1]);
+        v[2] = fmaf(uz[j], tz, v[2]);
+        v[3] = fmaf(ux[j], ty, v[3]);
+        v[4] = fmaf(uy[j], tz, v[4]);
+        v[5] = fmaf(uz[j], tx, v[5]);
       }
     }
   }

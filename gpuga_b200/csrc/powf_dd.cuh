@@ -9,7 +9,8 @@
 //
 //   x = 2^e m, m in [sqrt(1/2), sqrt(2)),  f = m - 1 (exact),
 //   s = f / (2 + f) as s_h + s_l (reciprocal estimate, exact FMA residual),
-//   log2(m) = (2/ln 2) atanh(s) = K (s + s^3/3 + s^5/5 + ... + s^11/11),  |s| <= 0.1716,
+//   log2(m) = (2/ln 2) atanh(s) = K (s + s^3/3 + s^5/5 + ... + s^9/9),  |s| <= 0.1716
+//     (the omitted terms: below K s^11 / 11 < 1.1e-9 absolute),
 //   L = e + log2(m) (Fast2Sum: |e| >= 1 > |log2 m| or e = 0),
 //   t = y L (exact FMA residual),  2^t = 2^k 2^r, k = rint(t_h), |r| <= 1/2,
 //   2^r = sum_{i<=7} (r ln 2)^i / i!  (Taylor series; truncation < 6e-9 relative).
@@ -61,7 +62,9 @@ GPUGA_HD float pdd_rcp(float t) {
 #endif
 }
 
-GPUGA_HD float powf_dd(float x, float y, float y_lo = 0.0f) {
+// LO: the exponent carries a remainder, y + y_lo (the two- and three-argument forms below).
+template <bool LO>
+GPUGA_HD float powf_dd_t(float x, float y, float y_lo) {
 #ifndef __CUDA_ARCH__
   if (x != x) return x;  // NaN (on the device: selected at the end, without a branch)
 #endif
@@ -78,11 +81,10 @@ GPUGA_HD float powf_dd(float x, float y, float y_lo = 0.0f) {
   float res = fmaf(-s_h, t, f);
   res = fmaf(-s_h, t_lo, res);
   const float s_l = res * rc;
-  // log2(m) = K s + K s^3 (1/3 + s^2/5 + s^4/7 + s^6/9 + s^8/11), K = 2/ln 2 = K_h + K_l
+  // log2(m) = K s + K s^3 (1/3 + s^2/5 + s^4/7 + s^6/9), K = 2/ln 2 = K_h + K_l
   const float K_h = 2.885390043258667f, K_l = 3.851926067000022e-08f;
   const float s2 = s_h * s_h;
-  float p = fmaf(s2, 1.0f / 11.0f, 1.0f / 9.0f);
-  p = fmaf(s2, p, 1.0f / 7.0f);
+  float p = fmaf(s2, 1.0f / 9.0f, 1.0f / 7.0f);
   p = fmaf(s2, p, 1.0f / 5.0f);
   p = fmaf(s2, p, 1.0f / 3.0f);
   const float q = s_h * s2 * p;
@@ -99,7 +101,7 @@ GPUGA_HD float powf_dd(float x, float y, float y_lo = 0.0f) {
   const float t_h = y * L_h;
   float t_l = fmaf(y, L_h, -t_h);
   t_l = fmaf(y, L_l, t_l);
-  t_l = fmaf(y_lo, L_h, t_l);  // y = y + y_lo when the exponent itself is a rounded FP64 value
+  if (LO) t_l = fmaf(y_lo, L_h, t_l);  // y = y + y_lo when the exponent itself is a rounded FP64 value
   // 2^t = 2^k 2^r (out of range: selected away at the end, no branch)
   const float k = rintf(t_h);
   const float r = (t_h - k) + t_l;
@@ -118,5 +120,8 @@ GPUGA_HD float powf_dd(float x, float y, float y_lo = 0.0f) {
   return out;
 #endif
 }
+
+GPUGA_HD float powf_dd(float x, float y) { return powf_dd_t<false>(x, y, 0.0f); }
+GPUGA_HD float powf_dd(float x, float y, float y_lo) { return powf_dd_t<true>(x, y, y_lo); }
 
 }  // namespace gpuga
