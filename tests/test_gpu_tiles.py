@@ -55,3 +55,28 @@ def test_every_tile_gives_the_same_bits(golden, tmp_path):
                 assert np.all(codes[:Ncf] == tiles) and np.all(codes[Ncf:] == 0)
             else:
                 assert np.all((codes[:Ncf] >= 1) & (codes[:Ncf] <= 5)) and np.all(codes[Ncf:] == 0)
+
+
+def test_fast_form_for_bonds_inside_r1_gives_the_same_bits():
+    """Atoms whose bonds all lie inside r1 take a form without the cutoff terms when every lane of
+    their warp agrees (tersoff_atom's vote).  With r1 a fitted parameter in [2.5, 2.9] A, many
+    atoms of the diamond cells have bonds beyond some individuals' r1, so which form an atom takes
+    depends on the atoms and individuals that share its warp: the tiles (different warp
+    compositions in force items) and an individual alone or in a population (different lanes in
+    energy/virial items) must still give identical bits.  Reference: the cutoff function and its
+    use, minimal_tersoff.cu:77-90 and 191-316."""
+    data = synth.make(2, Nc=16, seed=31)
+    data["pmin"][7], data["pmax"][7] = 2.5, 2.9  # r1 per individual (r2 stays 3.2)
+    with Fitness(arrays=data) as e0:
+        data = synth.fill_targets(data, lambda _d, p: e0.find_force64(p))
+    P = 40
+    pop = np.random.default_rng(11).uniform(0, 1, size=(P, len(data["pmin"]))).astype(np.float32)
+    ref = _run("arrays", data, 1, P, pop)
+    for tiles in (2, 3, 4):
+        got = _run("arrays", data, tiles, P, pop)
+        for a, b in zip(got[:5], ref[:5]):
+            assert np.array_equal(a, b), f"tiles={tiles}: results differ from the fixed rule"
+    with Fitness(arrays=data, tiles=1) as e:
+        for i in (0, 17, 39):
+            alone = np.asarray(e.compute(1, pop[i:i + 1], path=PATH_BATCHED))
+            assert alone[0] == ref[0][i], f"individual {i}: alone {alone[0]!r} vs in the population {ref[0][i]!r}"
